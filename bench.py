@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark: 3D Voronoi cells/s on B200 (meshless_voronoi per-cell construction path).
+
+A step is one complete tessellation of the workload: generator prep + uniform grid,
+cell construction (neighbour shells, clipping, exact predicates, integrals), face
+ordering and the cell -> face CSR.  Default workload: 256^3 = 16,777,216 i.i.d.
+uniform generators in the periodic unit box (seeded, synthetic).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision filtered|fp64]
+                  [--workload poisson_256|lattice_64|jitter_32] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank tessellates its own
+independently seeded generator set (weak scaling, no collective on the data path);
+value = all ranks' cells / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D Voronoi cells/s on 1 B200: FP32-filtered batched vs plain FP64, exact topology"
+HBM_PEAK_FALLBACK = 6650.0
+# algorithmic bytes (generator read + cell outputs + owned faces + CSR entries)
+BYTES_GEN, BYTES_CELL, BYTES_FACE, BYTES_CONN = 24, 40, 68, 4
+
+
+def workload(name: str, seed: int):
+    from meshless_voro_b200 import workloads as W
+    if name == "poisson_256":
+        w = W.poisson(256 ** 3, seed=seed, periodic=True)
+        w["name"] = "poisson_256^3_periodic_unit_box"
+    elif name == "lattice_64":
+        w = W.exact_lattice(64)
+    elif name == "jitter_32":
+        w = W.jittered_lattice_32(seed)
+    elif name.startswith("poisson_"):
+        n = int(name.split("_")[1]) ** 3
+        w = W.poisson(n, seed=seed, periodic=True)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return w
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_PEAK_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(w, budget_s=12.0, threads=None):
+    """The oracle (C++ restatement of the reference algorithm) with OpenMP on all host
+    cores, on a random sample of the workload's cells; extrapolated to the full set."""
+    from oracle import oracle as O
+    g, n = w["generators"], len(w["generators"])
+    threads = threads or os.cpu_count()
+    rng = np.random.default_rng(99)
+    kw = dict(dim=w["dimensionality"], periodic=w["periodic"], nthreads=threads,
+              flags=O.NO_CSR)
+    t0 = time.perf_counter()
+    O.build(g, w["anchor"], w["width"], mask=np.zeros(n, dtype=bool), **kw)
+    t_fixed = time.perf_counter() - t0            # grid build + flatten (serial)
+    m = min(n, 20000)
+    mask = np.zeros(n, dtype=bool)
+    mask[rng.choice(n, m, replace=False)] = True
+    t0 = time.perf_counter()
+    O.build(g, w["anchor"], w["width"], mask=mask, **kw)
+    rate = m / max(time.perf_counter() - t0 - t_fixed, 1e-6)
+    m = int(min(n, max(m, rate * budget_s)))
+    mask[:] = False
+    mask[rng.choice(n, m, replace=False)] = True
+    t0 = time.perf_counter()
+    r = O.build(g, w["anchor"], w["width"], mask=mask, **kw)
+    t_cells = time.perf_counter() - t0 - t_fixed
+    assert r.status == 0
+    full = t_fixed + t_cells * n / m
+    return {"value": n / full, "unit": "cells/s", "cores": threads, "kind": "port",
+            "sample": f"{m} random cells of the same {n}-generator workload "
+                      f"({t_cells:.1f} s of cell work + {t_fixed:.1f} s serial grid build, "
+                      f"extrapolated to all cells)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w = workload(args.workload, seed=3)
+    n = len(w["generators"])
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(w, budget_s=2.0)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(w, budget_s=args.cpu_budget)["value"])
+    cb = cpu_baseline(w, budget_s=args.cpu_budget)
+    v = float(np.median(vals))
+    line = {"metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": w["name"], "n_generators": n, "periodic": w["periodic"],
+                       "cache": "inputs larger than L2"},
+            "cpu_baseline": {**cb, "value": v},
+            "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "Rust reference cannot be built here (no cargo); the C++ restatement "
+                    "of its algorithm (oracle/) runs on all host cores"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poisson_256")
+    ap.add_argument("--precision", default="filtered", choices=["filtered", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 side run")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import meshless_voro_b200 as mv
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev,
+                                timeout=__import__("datetime").timedelta(seconds=120))
+
+    w = workload(args.workload, seed=3 + rank)
+    n = len(w["generators"])
+    g_host = torch.from_numpy(np.ascontiguousarray(w["generators"])).pin_memory()
+    g_dev = g_host.to(dev)
+    ctx = mv.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step(precision):
+        return ctx.build_device(g_dev.data_ptr(), 0, n, w["anchor"], w["width"],
+                                w["dimensionality"], w["periodic"], precision=precision,
+                                stream=sp)
+
+    def timed(precision, steps):
+        for _ in range(args.warmup):
+            step(precision)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cells_ms, stats, out = [], None, None
+        e0.record(stream)
+        for _ in range(steps):
+            out = step(precision)
+            stats = ctx.last_stats()
+            cells_ms.append(stats["ms_cells"])
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        if world > 1:
+            dist.barrier()
+        return ms, float(np.mean(cells_ms)), stats, out
+
+    with ClockSampler(local) as clk:
+        ms, cells_ms, stats, out = timed(args.precision, args.steps)
+    clocks = clk.summary()
+    F, Cn = int(out.n_faces), int(out.n_connections)
+    value = world * n / (ms * 1e-3)
+
+    # plain FP64 kernel side by side (same workload, same step)
+    other = None
+    if not args.no_compare:
+        o_prec = "fp64" if args.precision == "filtered" else "filtered"
+        o_ms, o_cells_ms, o_stats, _ = timed(o_prec, max(2, args.steps // 2))
+        other = {"precision": o_prec, "value": world * n / (o_ms * 1e-3),
+                 "ms_per_step": o_ms, "cells_kernel_ms": o_cells_ms,
+                 "f32_undecided": o_stats["f32_undecided"], "exact_tests": o_stats["exact_tests"]}
+
+    # end to end through the C ABI with host buffers (pinned input, results to pinned host)
+    e2e = None
+    if not args.no_e2e:
+        from meshless_voro_b200 import _native as NN
+        import ctypes as C
+        opts = mv.voronoi.make_options(args.precision, stream=sp)
+        a3 = (C.c_double * 3)(*w["anchor"])
+        w3 = (C.c_double * 3)(*w["width"])
+        hv = C.POINTER(NN.HostVoronoi)()
+
+        def e2e_step():
+            rc = NN.lib().mv_context_build(ctx.handle, C.c_void_p(g_host.data_ptr()), None, n,
+                                           a3, w3, w["dimensionality"], int(w["periodic"]),
+                                           C.byref(opts), C.byref(hv))
+            NN.check(rc)
+            return hv.contents
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            h = e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e_ms = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        d2h = (8 + 24 + 8 + 8 + 4) * n + (4 + 4 + 8 + 24 + 24 + 1) * int(h.n_faces) + 4 * int(h.n_connections)
+        e2e = {"value": world * n / (e_ms * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
+
+    peak, peak_kind = measured_peaks()
+    alg_bytes = BYTES_GEN * n + BYTES_CELL * n + BYTES_FACE * F + BYTES_CONN * Cn
+    achieved = alg_bytes / (cells_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "kernel": "mv::cells_kernel", "alg_bytes_per_launch": alg_bytes,
+                "kernel_ms": cells_ms}
+
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(workload(args.workload, seed=3), budget_s=args.cpu_budget)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": w["name"], "n_generators": n, "periodic": w["periodic"],
+                           "precision": args.precision, "parallelism": f"weak{world}",
+                           "cache": "inputs larger than L2 (403 MB generators)"},
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
+                "gpu_launches": int(stats["kernel_launches"]) * args.steps,
+                "clocks": clocks,
+                "phases_ms": {"grid": stats["ms_grid"], "cells": stats["ms_cells"],
+                              "finalize": stats["ms_finalize"]},
+                "counts": {"faces": F, "connections": Cn,
+                           "neighbours_clipped": stats["neighbours_clipped"],
+                           "planes_added": stats["planes_added"],
+                           "f32_undecided": stats["f32_undecided"],
+                           "exact_tests": stats["exact_tests"],
+                           "extra_shells": stats["extra_shells"],
+                           "overflow_cells": stats["overflow_cells"],
+                           "serial_rings": stats["serial_rings"]},
+                "side_by_side": other}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

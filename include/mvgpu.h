@@ -1,0 +1,178 @@
+/* mvgpu.h -- C ABI of the B200 (sm_100a) meshless Voronoi cell-construction library.
+ *
+ * Drop-in boundary for the per-cell construction path of the Rust crate
+ * meshless_voronoi 0.7.2.  Each entry point below names the reference interface it
+ * replaces (file:line in the crate).  All functions are thread-safe per context; a
+ * context must not be used by two host threads at once.
+ *
+ * Layouts follow the reference: generators are `&[DVec3]` (n x 3 doubles, 24-byte
+ * stride); cells, faces and cell->face connections come out in the reference's
+ * order (faces grouped by their left cell in cell order, inside a cell in clipping-
+ * plane order; connections per cell in increasing face index, voronoi.rs:241-263).
+ * Indices are int32 (a tessellation holds fewer than 2^31 generators and faces);
+ * a Rust binding widens them to usize.
+ */
+#ifndef MVGPU_H
+#define MVGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference panics where these are returned) ---- */
+enum {
+  MV_OK = 0,
+  MV_ERR_ARG = 1,          /* invalid argument                                        */
+  MV_ERR_DEGENERATE = 2,   /* duplicate generators: convex_cell.rs:325-329, 342       */
+  MV_ERR_RING = 3,         /* no ring extension found: convex_cell.rs:428             */
+  MV_ERR_DET = 4,          /* singular 3-plane intersection: geometry.rs:70           */
+  MV_ERR_CAPACITY = 5,     /* a cell outgrew the largest device capacity tier         */
+  MV_ERR_CUDA = 6,         /* a CUDA runtime call failed                              */
+  MV_ERR_NO_DEVICE = 7,    /* no usable CUDA device                                   */
+  MV_ERR_OOM = 8           /* device or pinned-host allocation failed                 */
+};
+
+/* ---- predicate precision ---- */
+enum {
+  MV_PRECISION_FP64 = 0,      /* every clip test in f64, as the reference            */
+  MV_PRECISION_FILTERED = 1   /* f32 test under a proven bound, f64 + exact fallback */
+};
+
+/* ---- which faces a build emits ---- */
+enum {
+  MV_FACES_OWNED = 0,  /* Voronoi::build and compute_face_integrals_sym: one per face */
+  MV_FACES_ALL = 1     /* compute_face_integrals: every face of every built cell      */
+};
+
+/* ---- dimensionality (voronoi.rs:31-40) ---- */
+enum { MV_DIM_1 = 1, MV_DIM_2 = 2, MV_DIM_3 = 3 };
+
+typedef struct mv_options {
+  int precision;                 /* MV_PRECISION_*                                   */
+  int face_mode;                 /* MV_FACES_*                                       */
+  double points_per_grid_cell;   /* 0: library default                               */
+  double initial_radius;         /* first neighbour shell, in mean spacings; 0: default */
+  void* stream;                  /* cudaStream_t to run on; NULL: the context stream */
+} mv_options;
+
+/* Per-build counters (escalations and retries). */
+typedef struct mv_build_stats {
+  int64_t cells_built;           /* active cells constructed                         */
+  int64_t neighbours_clipped;    /* half-spaces tested against a cell                */
+  int64_t planes_added;          /* half-spaces that removed at least one vertex     */
+  int64_t f32_undecided;         /* filtered mode: f32 tests that fell back to f64   */
+  int64_t exact_tests;           /* exact integer in-sphere evaluations              */
+  int64_t extra_shells;          /* neighbour-shell expansions beyond the first      */
+  int64_t overflow_cells;        /* cells re-run in the large capacity tier          */
+  int64_t serial_rings;          /* rings rebuilt by the serial fallback             */
+  int64_t device_bytes;          /* device workspace held by the context             */
+  int64_t kernel_launches;       /* library kernels launched by the build            */
+  double ms_grid;                /* device time: generator prep + uniform grid       */
+  double ms_cells;               /* device time: cell construction kernels           */
+  double ms_finalize;            /* device time: face ordering + cell->face CSR      */
+} mv_build_stats;
+
+/* Device-resident result of a build.  Pointers are owned by the context and stay
+ * valid until the next build on it or mv_context_destroy.  Arrays are indexed by
+ * original generator index; inactive cells of a partial build hold zeros. */
+typedef struct mv_device_voronoi {
+  int64_t n_cells, n_faces, n_connections;
+  double* cell_volume;        /* [n]                                                   */
+  double* cell_centroid;      /* [n][3]                                                */
+  double* cell_safety_radius; /* [n]                                                   */
+  int64_t* cell_face_offset;  /* [n]  offset into cell_face_connections                */
+  int32_t* cell_face_count;   /* [n]                                                   */
+  int32_t* face_left;         /* [F]                                                   */
+  int32_t* face_right;        /* [F]  -1: boundary face (right() == None)              */
+  double* face_area;          /* [F]                                                   */
+  double* face_centroid;      /* [F][3]                                                */
+  double* face_normal;        /* [F][3] clipping-plane normal, towards the left cell   */
+  uint8_t* face_shift_code;   /* [F]  13: no shift; else (mx+1)+3(my+1)+9(mz+1)        */
+  int32_t* cell_face_connections; /* [C]                                               */
+  int64_t error_cell;         /* first failing cell for error statuses, else -1        */
+} mv_device_voronoi;
+
+/* Host result (same arrays, host memory).  VoronoiCell::loc() is the generator with
+ * unused dims zeroed for built cells and 0 for inactive ones (voronoi_cell.rs:107);
+ * VoronoiFace::shift() is mv_shift_from_code(face_shift_code[f]). */
+typedef struct mv_voronoi {
+  int64_t n_cells, n_faces, n_connections;
+  int dimensionality, periodic;
+  double anchor[3], width[3];   /* normalised simulation volume (voronoi.rs:200-210)  */
+  double* cell_volume;
+  double* cell_centroid;
+  double* cell_safety_radius;
+  int64_t* cell_face_offset;
+  int32_t* cell_face_count;
+  int32_t* face_left;
+  int32_t* face_right;
+  double* face_area;
+  double* face_centroid;
+  double* face_normal;
+  uint8_t* face_shift_code;
+  int32_t* cell_face_connections;
+  int64_t error_cell;           /* first failing cell for error statuses, else -1     */
+  void* _owner;                 /* internal                                           */
+} mv_voronoi;
+
+typedef struct mv_context mv_context;
+
+/* Default options: filtered precision, owned faces, context stream. */
+void mv_options_default(mv_options* opts);
+
+/* Human-readable message for a status code (never NULL). */
+const char* mv_strerror(int status);
+
+/* Library version string. */
+const char* mv_version(void);
+
+/* A context owns a CUDA stream, the device workspace (grown on demand and reused)
+ * and a pinned host arena for results.  device < 0 selects the current device. */
+int mv_context_create(int device, mv_context** ctx);
+void mv_context_destroy(mv_context* ctx);
+
+/* Counters of the last build on the context. */
+int mv_context_last_stats(const mv_context* ctx, mv_build_stats* out);
+
+/* Replaces Voronoi::build (voronoi.rs:151-159) and Voronoi::build_partial
+ * (voronoi.rs:181-190) with device-resident inputs and outputs.
+ * d_generators: device [n][3] doubles; d_mask: device [n] bytes (nonzero == true) or
+ * NULL for a full build.  Returns when the result is complete on the device. */
+int mv_context_build_device(mv_context* ctx, const double* d_generators, const uint8_t* d_mask,
+                            int64_t n, const double anchor[3], const double width[3],
+                            int dimensionality, int periodic, const mv_options* opts,
+                            mv_device_voronoi* out);
+
+/* Same as mv_context_build_device with host inputs; the result is copied into the
+ * context's pinned host arena (valid until the next build on the context).  *out
+ * is owned by the context: do not pass it to mv_voronoi_free. */
+int mv_context_build(mv_context* ctx, const double* generators, const uint8_t* mask, int64_t n,
+                     const double anchor[3], const double width[3], int dimensionality,
+                     int periodic, const mv_options* opts, mv_voronoi** out);
+
+/* Stand-alone Voronoi::build (voronoi.rs:151-159): host in, host out, on the current
+ * device with a temporary context.  Free the result with mv_voronoi_free. */
+int mv_voronoi_build(const double* generators, int64_t n, const double anchor[3],
+                     const double width[3], int dimensionality, int periodic,
+                     const mv_options* opts, mv_voronoi** out);
+
+/* Stand-alone Voronoi::build_partial (voronoi.rs:181-190). */
+int mv_voronoi_build_partial(const double* generators, const uint8_t* mask, int64_t n,
+                             const double anchor[3], const double width[3], int dimensionality,
+                             int periodic, const mv_options* opts, mv_voronoi** out);
+
+void mv_voronoi_free(mv_voronoi* v);
+
+/* The reference's shift vector for a face shift code (rtree_nn.rs:27-33): component i
+ * is m_i * width_i for m_i != 0 and -0.0 for m_i == 0, with (m_x, m_y, m_z) decoded
+ * from code = (m_x+1) + 3(m_y+1) + 9(m_z+1).  Code 13 (no shift) gives all -0.0. */
+void mv_shift_from_code(int code, const double width[3], double out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MVGPU_H */

@@ -1,0 +1,65 @@
+"""Build recipe of the CUDA library ``libmvgpu.so`` (sm_100a).
+
+The library is built in-tree into ``meshless_voro_b200/_lib/`` so it travels with the
+source tree.  f64 code is compiled without FMA contraction (``--fmad=false``) and
+with IEEE division and square root, which keeps every f64 value equal to the
+reference crate's.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIB_DIR, "libmvgpu.so")
+
+SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu"]
+HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h"]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
+    "-shared", "-cudart", "shared",
+]
+
+
+def _inputs():
+    files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    files.append(os.path.join(INCLUDE, "mvgpu.h"))
+    files.append(os.path.abspath(__file__))
+    return files
+
+
+def is_stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in _inputs())
+
+
+def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
+    """Compile libmvgpu.so for sm_100a if it is missing or stale; return its path."""
+    if not force and not is_stale():
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    tmp = LIB + f".tmp{os.getpid()}"
+    cmd = [NVCC, *NVCC_FLAGS, *(extra_flags or []), "-I", INCLUDE,
+           *[os.path.join(CSRC, f) for f in SOURCES], "-o", tmp]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    extra = [a for a in sys.argv[1:] if a.startswith("-X") or a.startswith("--")]
+    extra = [a for a in extra if a != "--force"]
+    print(build(force="--force" in sys.argv, verbose=True, extra_flags=extra))

@@ -1,0 +1,784 @@
+// mv_api.cu -- host orchestration and the C ABI (include/mvgpu.h).
+//
+// Replaces the orchestration of Voronoi::build / build_partial (voronoi.rs:151-263):
+// dimension normalisation, SimulationBoundary::cuboid, the neighbour structure, the
+// per-cell construction, flatten and finalize.  Host-side f64 arithmetic (the
+// boundary planes) is compiled without FMA contraction, like the device code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "../../include/mvgpu.h"
+#include "mv_geom.cuh"
+#include "mv_internal.h"
+
+namespace mv {
+// mv_cells.cu
+cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
+int cells_blocks_per_sm_fast(int precision);
+int cells_blocks_per_sm_large(int precision);
+// mv_grid.cu
+void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
+                 double* ext, int* bad, cudaStream_t st);
+void launch_grid(const double* gen, int n, const int G[3], const double a[3], const double inv[3],
+                 int32_t* cid, int32_t* count, int32_t* start, int32_t* fill, double* sx, double* sy,
+                 double* sz, int32_t* sid, long long* scan_tmp, cudaStream_t st);
+size_t scan_tmp_elems(int64_t n);
+void scan_i32_to_i64(const int32_t* in, int64_t n, int64_t* out, long long* tmp, cudaStream_t st);
+void launch_reorder(const FaceArrays& stage, int64_t F, const int64_t* stage_off,
+                    const int64_t* face_off, const FaceArrays& out, cudaStream_t st);
+void launch_csr_counts(const FaceArrays& f, int64_t F, const int32_t* face_count, int n,
+                       int32_t* in_count, int32_t* conn_count, cudaStream_t st);
+void launch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, const int64_t* conn_off,
+                     const int32_t* in_count, int32_t* cursor, int n, int32_t* conn, cudaStream_t st);
+}  // namespace mv
+
+using namespace mv;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Workspace {
+  DevBuf in_xyz, in_mask;
+  DevBuf gen, sx, sy, sz, sid, cid;
+  DevBuf cell_count, cell_start, cell_fill, scan_tmp;
+  DevBuf volume, centroid, sr, face_count, stage_off, face_off;
+  DevBuf in_count, conn_count, conn_off, cursor, conn;
+  DevBuf st_left, st_right, st_area, st_cen, st_nrm, st_code;
+  DevBuf f_left, f_right, f_area, f_cen, f_nrm, f_code;
+  DevBuf ovf_a, ovf_b;
+  DevBuf counters;
+};
+
+}  // namespace
+
+struct mv_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  int sm_count = 0;
+  int bps_fast[2] = {0, 0};
+  int bps_large[2] = {0, 0};
+  Workspace ws;
+  size_t dev_bytes = 0;
+  double face_ratio_hint = 0.0;  // faces per cell needed by the last build
+  bool large_ran = false;
+  mv_build_stats last{};
+  // pinned host arena for mv_context_build
+  void* host = nullptr;
+  size_t host_cap = 0;
+  mv_voronoi hv{};
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return MV_OK;
+  if (e == cudaErrorMemoryAllocation) return MV_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return MV_ERR_NO_DEVICE;
+  return MV_ERR_CUDA;
+}
+
+#define MV_CUDA(call)                           \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+int ensure(mv_context* ctx, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return MV_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    ctx->dev_bytes -= b.cap;
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  size_t want = bytes + bytes / 8;  // headroom for slightly larger rebuilds
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMalloc(&b.p, bytes);
+    want = bytes;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return MV_ERR_OOM;
+  }
+  b.cap = want;
+  ctx->dev_bytes += want;
+  return MV_OK;
+}
+
+template <class T>
+T* P(DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+struct Setup {
+  double anchor[3], width[3];
+  int dim, periodic;
+  int G[3];
+  double gh[3], ginv[3], geps[3];
+  double R0;
+  double bn[6][3], bp[6][3], bd[6];
+  double iloc_a[3], iloc_inv[3];
+};
+
+// voronoi.rs:200-210 + boundary.rs:14-47 + the grid resolution.
+int make_setup(int64_t n, const double* anchor, const double* width, int dim, int periodic,
+               const mv_options& o, Setup* s) {
+  if (dim < 1 || dim > 3) return MV_ERR_ARG;
+  D3 a = {anchor[0], anchor[1], anchor[2]};
+  D3 w = {width[0], width[1], width[2]};
+  if (dim == 1) {
+    a.y = -0.5;
+    w.y = 1.0;
+  }
+  if (dim == 1 || dim == 2) {
+    a.z = -0.5;
+    w.z = 1.0;
+  }
+  const double aa[3] = {a.x, a.y, a.z}, ww[3] = {w.x, w.y, w.z};
+  for (int i = 0; i < 3; i++) {
+    if (!std::isfinite(aa[i]) || !std::isfinite(ww[i]) || !(ww[i] > 0.0)) return MV_ERR_ARG;
+    s->anchor[i] = aa[i];
+    s->width[i] = ww[i];
+  }
+  s->dim = dim;
+  s->periodic = periodic ? 1 : 0;
+  // SimulationBoundary::cuboid
+  D3 ba = a, bw = w;
+  if (periodic) {
+    ba.x -= bw.x;
+    bw.x *= 3.0;
+    if (dim >= 2) {
+      ba.y -= bw.y;
+      bw.y *= 3.0;
+    }
+    if (dim == 3) {
+      ba.z -= bw.z;
+      bw.z *= 3.0;
+    }
+  }
+  const D3 hi = add(ba, bw);
+  const D3 ns[6] = {{1.0, 0.0, 0.0}, {-1.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
+                    {0.0, -1.0, 0.0}, {0.0, 0.0, 1.0}, {0.0, 0.0, -1.0}};
+  for (int k = 0; k < 6; k++) {
+    const D3 p = (k & 1) ? hi : ba;
+    s->bn[k][0] = ns[k].x, s->bn[k][1] = ns[k].y, s->bn[k][2] = ns[k].z;
+    s->bp[k][0] = p.x, s->bp[k][1] = p.y, s->bp[k][2] = p.z;
+    s->bd[k] = dot(ns[k], p);
+  }
+  const D3 ia = sub(ba, bw);
+  s->iloc_a[0] = ia.x, s->iloc_a[1] = ia.y, s->iloc_a[2] = ia.z;
+  s->iloc_inv[0] = 1.0 / (3.0 * bw.x);
+  s->iloc_inv[1] = 1.0 / (3.0 * bw.y);
+  s->iloc_inv[2] = 1.0 / (3.0 * bw.z);
+  // uniform grid: ~points_per_grid_cell generators per cell, at most 2^24 cells
+  double vol = 1.0;
+  for (int i = 0; i < dim; i++) vol *= ww[i];
+  const double nn = (double)std::max<int64_t>(n, 1);
+  double ppc = o.points_per_grid_cell > 0 ? o.points_per_grid_cell : 2.2;
+  double h = std::pow(vol * ppc / nn, 1.0 / dim);
+  for (;;) {
+    int64_t cells = 1;
+    for (int i = 0; i < 3; i++) {
+      int G = 1;
+      if (i < dim) G = (int)std::max(1.0, std::min(std::floor(ww[i] / h), 4096.0));
+      s->G[i] = G;
+      cells *= G;
+    }
+    if (cells <= (1ll << 24)) break;
+    h *= 1.25;
+  }
+  for (int i = 0; i < 3; i++) {
+    s->gh[i] = ww[i] / s->G[i];
+    s->ginv[i] = s->G[i] / ww[i];
+    s->geps[i] = 1e-9 * s->gh[i] + 1e-13 * (std::fabs(aa[i]) + ww[i]);
+  }
+  const double spacing = std::pow(vol / nn, 1.0 / dim);
+  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.6 : (dim == 2 ? 2.4 : 2.2));
+  s->R0 = r0 * spacing;
+  return MV_OK;
+}
+
+double face_ratio(int dim, int face_mode) {
+  if (dim == 3) return face_mode == MV_FACES_ALL ? 17.5 : 10.5;
+  if (dim == 2) return face_mode == MV_FACES_ALL ? 7.5 : 4.5;
+  return 2.5;
+}
+
+int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mask, int64_t n,
+                      const double* anchor, const double* width, int dim, int periodic,
+                      const mv_options* opts_in, mv_device_voronoi* out) {
+  mv_options o;
+  mv_options_default(&o);
+  if (opts_in) o = *opts_in;
+  if (!out || n < 0 || (n > 0 && !d_xyz)) return MV_ERR_ARG;
+  if (n >= (int64_t)(0xffffffffu / 27u)) return MV_ERR_ARG;  // neighbour tie key range
+  if (o.precision != MV_PRECISION_FP64 && o.precision != MV_PRECISION_FILTERED) return MV_ERR_ARG;
+  if (o.face_mode != MV_FACES_OWNED && o.face_mode != MV_FACES_ALL) return MV_ERR_ARG;
+  Setup s;
+  int rc = make_setup(n, anchor, width, dim, periodic, o, &s);
+  if (rc) return rc;
+  MV_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  Workspace& W = ctx->ws;
+  const int ni = (int)n;
+  const int64_t ncell = (int64_t)s.G[0] * s.G[1] * s.G[2];
+  const size_t N = (size_t)std::max<int64_t>(n, 1);
+
+  // ---- workspace ----
+  int e = 0;
+  e |= ensure(ctx, W.gen, 24 * N);
+  e |= ensure(ctx, W.sx, 8 * N);
+  e |= ensure(ctx, W.sy, 8 * N);
+  e |= ensure(ctx, W.sz, 8 * N);
+  e |= ensure(ctx, W.sid, 4 * N);
+  e |= ensure(ctx, W.cid, 4 * N);
+  e |= ensure(ctx, W.cell_count, 4 * (ncell + 1));
+  e |= ensure(ctx, W.cell_start, 4 * (ncell + 1));
+  e |= ensure(ctx, W.cell_fill, 4 * (ncell + 1));
+  e |= ensure(ctx, W.scan_tmp, 8 * (scan_tmp_elems(std::max<int64_t>(ncell + 1, N)) + 64));
+  e |= ensure(ctx, W.volume, 8 * N);
+  e |= ensure(ctx, W.centroid, 24 * N);
+  e |= ensure(ctx, W.sr, 8 * N);
+  e |= ensure(ctx, W.face_count, 4 * N);
+  e |= ensure(ctx, W.stage_off, 8 * N);
+  e |= ensure(ctx, W.face_off, 8 * (N + 1));
+  e |= ensure(ctx, W.in_count, 4 * N);
+  e |= ensure(ctx, W.conn_count, 4 * N);
+  e |= ensure(ctx, W.conn_off, 8 * (N + 1));
+  e |= ensure(ctx, W.cursor, 4 * N);
+  e |= ensure(ctx, W.ovf_a, 4 * N);
+  e |= ensure(ctx, W.ovf_b, 4 * N);
+  e |= ensure(ctx, W.counters, sizeof(DevCounters));
+  if (e) return MV_ERR_OOM;
+  double ratio = std::max(face_ratio(s.dim, o.face_mode), ctx->face_ratio_hint);
+  int64_t face_cap = (int64_t)(ratio * (double)n) + 4096;
+
+  DevCounters* C = P<DevCounters>(W.counters);
+  mv_build_stats stats{};
+  int64_t launches = 0;
+  int64_t F = 0;
+  for (int attempt = 0;; attempt++) {
+    size_t FC = (size_t)face_cap;
+    e = 0;
+    e |= ensure(ctx, W.st_left, 4 * FC);
+    e |= ensure(ctx, W.st_right, 4 * FC);
+    e |= ensure(ctx, W.st_area, 8 * FC);
+    e |= ensure(ctx, W.st_cen, 24 * FC);
+    e |= ensure(ctx, W.st_nrm, 24 * FC);
+    e |= ensure(ctx, W.st_code, FC);
+    if (e) return MV_ERR_OOM;
+    face_cap = (int64_t)std::min(W.st_left.cap / 4, W.st_code.cap);
+    face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_area.cap / 8));
+    face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_cen.cap / 24));
+
+    // ---- clear counters ----
+    MV_CUDA(cudaMemsetAsync(C, 0, sizeof(DevCounters), st));
+    MV_CUDA(cudaMemsetAsync(C->ext_keys, 0xff, 3 * sizeof(unsigned long long), st));
+    MV_CUDA(cudaMemsetAsync(W.cell_count.p, 0, 4 * (ncell + 1), st));
+    MV_CUDA(cudaMemsetAsync(W.cell_fill.p, 0, 4 * (ncell + 1), st));
+
+    // ---- generators + grid (replaces build_rtree, rtree_nn.rs:6-8) ----
+    MV_CUDA(cudaEventRecord(ctx->ev[0], st));
+    launches = 7;  // prep, extent, cell index, 3 scan kernels, scatter
+    launch_prep(d_xyz, ni, s.dim, P<double>(W.gen), C->ext_keys, C->ext, &C->bad_input, st);
+    launch_grid(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
+                P<int32_t>(W.cell_count), P<int32_t>(W.cell_start), P<int32_t>(W.cell_fill),
+                P<double>(W.sx), P<double>(W.sy), P<double>(W.sz), P<int32_t>(W.sid),
+                P<long long>(W.scan_tmp), st);
+
+    // ---- cells ----
+    Job J;
+    std::memset(&J, 0, sizeof(J));
+    J.gen = P<double>(W.gen);
+    J.sx = P<double>(W.sx);
+    J.sy = P<double>(W.sy);
+    J.sz = P<double>(W.sz);
+    J.sid = P<int32_t>(W.sid);
+    J.cell_start = P<int32_t>(W.cell_start);
+    J.mask = d_mask;
+    J.n = ni;
+    J.dim = s.dim;
+    J.periodic = s.periodic;
+    J.face_mode = o.face_mode;
+    J.precision = o.precision;
+    for (int i = 0; i < 3; i++) {
+      J.G[i] = s.G[i];
+      J.ga[i] = s.anchor[i];
+      J.gw[i] = s.width[i];
+      J.gh[i] = s.gh[i];
+      J.ginv[i] = s.ginv[i];
+      J.geps[i] = s.geps[i];
+      J.iloc_a[i] = s.iloc_a[i];
+      J.iloc_inv[i] = s.iloc_inv[i];
+    }
+    J.ext = C->ext;
+    J.R0 = s.R0;
+    for (int k = 0; k < 6; k++) {
+      for (int i = 0; i < 3; i++) J.bn[k][i] = s.bn[k][i], J.bp[k][i] = s.bp[k][i];
+      J.bd[k] = s.bd[k];
+    }
+    J.volume = P<double>(W.volume);
+    J.centroid = P<double>(W.centroid);
+    J.safety_radius = P<double>(W.sr);
+    J.face_count = P<int32_t>(W.face_count);
+    J.stage_off = P<int64_t>(W.stage_off);
+    J.f_left = P<int32_t>(W.st_left);
+    J.f_right = P<int32_t>(W.st_right);
+    J.f_area = P<double>(W.st_area);
+    J.f_centroid = P<double>(W.st_cen);
+    J.f_normal = P<double>(W.st_nrm);
+    J.f_code = P<uint8_t>(W.st_code);
+    J.face_counter = &C->face_counter;
+    J.face_cap = face_cap;
+    J.order = nullptr;
+    J.n_order = ni;
+    J.work_counter = &C->work[0];
+    J.ovf_list = P<int32_t>(W.ovf_a);
+    J.ovf_count = &C->ovf_count[0];
+    J.status = C->status;
+    J.stats = C->stats;
+    const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
+    MV_CUDA(cudaEventRecord(ctx->ev[1], st));
+    if (n > 0) {
+      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+      MV_CUDA(launch_cells(J, false, blocks, st));
+      launches++;
+    }
+    MV_CUDA(cudaEventRecord(ctx->ev[2], st));
+    bool large_ran = false;
+    DevCounters hc;
+    MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+    if (hc.bad_input) return MV_ERR_ARG;
+    unsigned novf = hc.ovf_count[0];
+    if (novf > 0 && !hc.status[STATUS_CODE]) {
+      // cells that outgrew the fast tier: the large tier rebuilds them
+      Job L = J;
+      L.order = P<int32_t>(W.ovf_a);
+      L.n_order = (int32_t)novf;
+      L.work_counter = &C->work[1];
+      L.ovf_list = P<int32_t>(W.ovf_b);
+      L.ovf_count = &C->ovf_count[1];
+      int blocks = ctx->sm_count * std::max(1, ctx->bps_large[pi]);
+      blocks = std::min<int>(blocks, (int)novf);
+      MV_CUDA(cudaEventRecord(ctx->ev[3], st));
+      MV_CUDA(launch_cells(L, true, blocks, st));
+      MV_CUDA(cudaEventRecord(ctx->ev[4], st));
+      launches++;
+      large_ran = true;
+      MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+      MV_CUDA(cudaStreamSynchronize(st));
+    }
+    ctx->large_ran = large_ran;
+    if (hc.status[STATUS_CODE]) {
+      std::memset(out, 0, sizeof(*out));
+      out->n_cells = n;
+      out->error_cell = hc.status[STATUS_CELL];
+      return hc.status[STATUS_CODE];
+    }
+    if (hc.ovf_count[1] > 0) return MV_ERR_CAPACITY;
+    if (hc.status[STATUS_FACE_OVERFLOW]) {
+      if (attempt >= 2) return MV_ERR_CAPACITY;
+      face_cap = (int64_t)(hc.face_counter * 1.15) + 4096;
+      ctx->face_ratio_hint = (double)face_cap / (double)std::max<int64_t>(n, 1);
+      continue;
+    }
+    F = (int64_t)hc.face_counter;
+    stats.cells_built = (int64_t)hc.stats[ST_CELLS];
+    stats.neighbours_clipped = (int64_t)hc.stats[ST_NEIGHBOURS];
+    stats.planes_added = (int64_t)hc.stats[ST_PLANES];
+    stats.f32_undecided = (int64_t)hc.stats[ST_F32_UNDECIDED];
+    stats.exact_tests = (int64_t)hc.stats[ST_EXACT];
+    stats.extra_shells = (int64_t)hc.stats[ST_SHELLS];
+    stats.overflow_cells = (int64_t)hc.stats[ST_OVERFLOW];
+    stats.serial_rings = (int64_t)hc.stats[ST_SERIAL_RING];
+    break;
+  }
+
+  // ---- flatten: faces in cell order (voronoi.rs:226) ----
+  {
+    size_t FF = (size_t)std::max<int64_t>(F, 1);
+    e = 0;
+    e |= ensure(ctx, W.f_left, 4 * FF);
+    e |= ensure(ctx, W.f_right, 4 * FF);
+    e |= ensure(ctx, W.f_area, 8 * FF);
+    e |= ensure(ctx, W.f_cen, 24 * FF);
+    e |= ensure(ctx, W.f_nrm, 24 * FF);
+    e |= ensure(ctx, W.f_code, FF);
+    if (e) return MV_ERR_OOM;
+  }
+  MV_CUDA(cudaEventRecord(ctx->ev[5], st));
+  scan_i32_to_i64(P<int32_t>(W.face_count), n, P<int64_t>(W.face_off), P<long long>(W.scan_tmp), st);
+  launches += 4;  // scan (3) + reorder
+  FaceArrays stage{P<int32_t>(W.st_left), P<int32_t>(W.st_right), P<double>(W.st_area),
+                   P<double>(W.st_cen), P<double>(W.st_nrm), P<uint8_t>(W.st_code)};
+  FaceArrays fin{P<int32_t>(W.f_left), P<int32_t>(W.f_right), P<double>(W.f_area),
+                 P<double>(W.f_cen), P<double>(W.f_nrm), P<uint8_t>(W.f_code)};
+  launch_reorder(stage, F, P<int64_t>(W.stage_off), P<int64_t>(W.face_off), fin, st);
+
+  // ---- Voronoi::finalize: cell -> face CSR (voronoi.rs:241-263) ----
+  int64_t Cn = 0;
+  if (o.face_mode == MV_FACES_OWNED) {
+    MV_CUDA(cudaMemsetAsync(W.in_count.p, 0, 4 * N, st));
+    MV_CUDA(cudaMemsetAsync(W.cursor.p, 0, 4 * N, st));
+    launch_csr_counts(fin, F, P<int32_t>(W.face_count), ni, P<int32_t>(W.in_count),
+                      P<int32_t>(W.conn_count), st);
+    scan_i32_to_i64(P<int32_t>(W.conn_count), n, P<int64_t>(W.conn_off), P<long long>(W.scan_tmp), st);
+    MV_CUDA(cudaMemcpyAsync(&Cn, P<int64_t>(W.conn_off) + n, 8, cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+    if (ensure(ctx, W.conn, 4 * (size_t)std::max<int64_t>(Cn, 1))) return MV_ERR_OOM;
+    launch_csr_fill(fin, F, P<int64_t>(W.face_off), P<int64_t>(W.conn_off), P<int32_t>(W.in_count),
+                    P<int32_t>(W.cursor), ni, P<int32_t>(W.conn), st);
+    launches += 7;  // in-count, conn-count, scan (3), fill, sort
+  }
+  MV_CUDA(cudaEventRecord(ctx->ev[6], st));
+  MV_CUDA(cudaGetLastError());
+  MV_CUDA(cudaStreamSynchronize(st));
+  stats.device_bytes = (int64_t)ctx->dev_bytes;
+  stats.kernel_launches = launches;
+  {
+    float t01 = 0.f, t12 = 0.f, t34 = 0.f, t56 = 0.f;
+    cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&t12, ctx->ev[1], ctx->ev[2]);
+    if (ctx->large_ran) cudaEventElapsedTime(&t34, ctx->ev[3], ctx->ev[4]);
+    cudaEventElapsedTime(&t56, ctx->ev[5], ctx->ev[6]);
+    stats.ms_grid = t01;
+    stats.ms_cells = t12 + t34;
+    stats.ms_finalize = t56;
+  }
+  ctx->last = stats;
+
+  out->n_cells = n;
+  out->n_faces = F;
+  out->n_connections = Cn;
+  out->cell_volume = P<double>(W.volume);
+  out->cell_centroid = P<double>(W.centroid);
+  out->cell_safety_radius = P<double>(W.sr);
+  out->cell_face_offset = o.face_mode == MV_FACES_OWNED ? P<int64_t>(W.conn_off) : nullptr;
+  out->cell_face_count = o.face_mode == MV_FACES_OWNED ? P<int32_t>(W.conn_count) : nullptr;
+  out->face_left = P<int32_t>(W.f_left);
+  out->face_right = P<int32_t>(W.f_right);
+  out->face_area = P<double>(W.f_area);
+  out->face_centroid = P<double>(W.f_cen);
+  out->face_normal = P<double>(W.f_nrm);
+  out->face_shift_code = P<uint8_t>(W.f_code);
+  out->cell_face_connections = o.face_mode == MV_FACES_OWNED ? P<int32_t>(W.conn) : nullptr;
+  out->error_cell = -1;
+  return MV_OK;
+}
+
+struct HostLayout {
+  size_t off[16];
+  size_t total;
+};
+
+HostLayout host_layout(int64_t n, int64_t F, int64_t Cn) {
+  const size_t sz[] = {8 * (size_t)n,  24 * (size_t)n, 8 * (size_t)n,  8 * (size_t)n,
+                       4 * (size_t)n,  4 * (size_t)F,  4 * (size_t)F,  8 * (size_t)F,
+                       24 * (size_t)F, 24 * (size_t)F, (size_t)F,      4 * (size_t)Cn};
+  HostLayout L;
+  size_t o = 0;
+  for (int i = 0; i < 12; i++) {
+    L.off[i] = o;
+    o += (sz[i] + 255) & ~(size_t)255;
+  }
+  L.total = o;
+  return L;
+}
+
+int copy_to_host(mv_context* ctx, const mv_device_voronoi& d, int64_t n, const Setup& s,
+                 cudaStream_t st, mv_voronoi* hv) {
+  HostLayout L = host_layout(n, d.n_faces, d.n_connections);
+  if (ctx->host_cap < L.total) {
+    if (ctx->host) cudaFreeHost(ctx->host);
+    ctx->host = nullptr;
+    ctx->host_cap = 0;
+    size_t want = L.total + L.total / 8 + 4096;
+    if (cudaHostAlloc(&ctx->host, want, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->host = nullptr;
+      return MV_ERR_OOM;
+    }
+    ctx->host_cap = want;
+  }
+  char* b = static_cast<char*>(ctx->host);
+  std::memset(hv, 0, sizeof(*hv));
+  hv->n_cells = n;
+  hv->n_faces = d.n_faces;
+  hv->n_connections = d.n_connections;
+  hv->dimensionality = s.dim;
+  hv->periodic = s.periodic;
+  for (int i = 0; i < 3; i++) hv->anchor[i] = s.anchor[i], hv->width[i] = s.width[i];
+  hv->cell_volume = (double*)(b + L.off[0]);
+  hv->cell_centroid = (double*)(b + L.off[1]);
+  hv->cell_safety_radius = (double*)(b + L.off[2]);
+  hv->cell_face_offset = (int64_t*)(b + L.off[3]);
+  hv->cell_face_count = (int32_t*)(b + L.off[4]);
+  hv->face_left = (int32_t*)(b + L.off[5]);
+  hv->face_right = (int32_t*)(b + L.off[6]);
+  hv->face_area = (double*)(b + L.off[7]);
+  hv->face_centroid = (double*)(b + L.off[8]);
+  hv->face_normal = (double*)(b + L.off[9]);
+  hv->face_shift_code = (uint8_t*)(b + L.off[10]);
+  hv->cell_face_connections = (int32_t*)(b + L.off[11]);
+  hv->error_cell = -1;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    if (!bytes || !src) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  const size_t N = (size_t)n, F = (size_t)d.n_faces, Cn = (size_t)d.n_connections;
+  MV_CUDA(cp(hv->cell_volume, d.cell_volume, 8 * N));
+  MV_CUDA(cp(hv->cell_centroid, d.cell_centroid, 24 * N));
+  MV_CUDA(cp(hv->cell_safety_radius, d.cell_safety_radius, 8 * N));
+  MV_CUDA(cp(hv->cell_face_offset, d.cell_face_offset, 8 * N));
+  MV_CUDA(cp(hv->cell_face_count, d.cell_face_count, 4 * N));
+  MV_CUDA(cp(hv->face_left, d.face_left, 4 * F));
+  MV_CUDA(cp(hv->face_right, d.face_right, 4 * F));
+  MV_CUDA(cp(hv->face_area, d.face_area, 8 * F));
+  MV_CUDA(cp(hv->face_centroid, d.face_centroid, 24 * F));
+  MV_CUDA(cp(hv->face_normal, d.face_normal, 24 * F));
+  MV_CUDA(cp(hv->face_shift_code, d.face_shift_code, F));
+  MV_CUDA(cp(hv->cell_face_connections, d.cell_face_connections, 4 * Cn));
+  MV_CUDA(cudaStreamSynchronize(st));
+  if (!d.cell_face_offset) {
+    hv->cell_face_offset = nullptr;
+    hv->cell_face_count = nullptr;
+    hv->cell_face_connections = nullptr;
+  }
+  return MV_OK;
+}
+
+int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int64_t n,
+                    const double* anchor, const double* width, int dim, int periodic,
+                    const mv_options* opts, mv_voronoi** out) {
+  if (!ctx || !out || n < 0 || (n > 0 && !xyz)) return MV_ERR_ARG;
+  mv_options o;
+  mv_options_default(&o);
+  if (opts) o = *opts;
+  Setup s;
+  int rc = make_setup(n, anchor, width, dim, periodic, o, &s);
+  if (rc) return rc;
+  MV_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  const size_t N = (size_t)std::max<int64_t>(n, 1);
+  if (ensure(ctx, ctx->ws.in_xyz, 24 * N) || ensure(ctx, ctx->ws.in_mask, N)) return MV_ERR_OOM;
+  if (n > 0) MV_CUDA(cudaMemcpyAsync(ctx->ws.in_xyz.p, xyz, 24 * (size_t)n, cudaMemcpyHostToDevice, st));
+  if (mask && n > 0) MV_CUDA(cudaMemcpyAsync(ctx->ws.in_mask.p, mask, (size_t)n, cudaMemcpyHostToDevice, st));
+  mv_device_voronoi d{};
+  d.error_cell = -1;
+  rc = build_device_impl(ctx, P<double>(ctx->ws.in_xyz), mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr,
+                         n, anchor, width, dim, periodic, &o, &d);
+  if (rc) {
+    std::memset(&ctx->hv, 0, sizeof(ctx->hv));
+    ctx->hv.n_cells = n;
+    ctx->hv.error_cell = d.error_cell;
+    *out = &ctx->hv;
+    return rc;
+  }
+  rc = copy_to_host(ctx, d, n, s, st, &ctx->hv);
+  if (rc) return rc;
+  *out = &ctx->hv;
+  return MV_OK;
+}
+
+struct OwnedVoronoi {
+  mv_voronoi v;
+  void* block;
+};
+
+int standalone(const double* xyz, const uint8_t* mask, int64_t n, const double* anchor,
+               const double* width, int dim, int periodic, const mv_options* opts,
+               mv_voronoi** out) {
+  if (!out) return MV_ERR_ARG;
+  *out = nullptr;
+  mv_context* ctx = nullptr;
+  int rc = mv_context_create(-1, &ctx);
+  if (rc) return rc;
+  mv_voronoi* hv = nullptr;
+  rc = build_host_impl(ctx, xyz, mask, n, anchor, width, dim, periodic, opts, &hv);
+  OwnedVoronoi* ov = new (std::nothrow) OwnedVoronoi();
+  if (!ov) {
+    mv_context_destroy(ctx);
+    return MV_ERR_OOM;
+  }
+  ov->v = *hv;
+  ov->block = nullptr;
+  ov->v._owner = ov;
+  if (rc == MV_OK) {
+    HostLayout L = host_layout(hv->n_cells, hv->n_faces, hv->n_connections);
+    ov->block = std::malloc(std::max<size_t>(L.total, 16));
+    if (!ov->block) {
+      delete ov;
+      mv_context_destroy(ctx);
+      return MV_ERR_OOM;
+    }
+    std::memcpy(ov->block, ctx->host, L.total);
+    char* b = static_cast<char*>(ov->block);
+    auto rebase = [&](void* p) -> char* {
+      return p ? b + (static_cast<char*>(p) - static_cast<char*>(ctx->host)) : nullptr;
+    };
+    ov->v.cell_volume = (double*)rebase(hv->cell_volume);
+    ov->v.cell_centroid = (double*)rebase(hv->cell_centroid);
+    ov->v.cell_safety_radius = (double*)rebase(hv->cell_safety_radius);
+    ov->v.cell_face_offset = (int64_t*)rebase(hv->cell_face_offset);
+    ov->v.cell_face_count = (int32_t*)rebase(hv->cell_face_count);
+    ov->v.face_left = (int32_t*)rebase(hv->face_left);
+    ov->v.face_right = (int32_t*)rebase(hv->face_right);
+    ov->v.face_area = (double*)rebase(hv->face_area);
+    ov->v.face_centroid = (double*)rebase(hv->face_centroid);
+    ov->v.face_normal = (double*)rebase(hv->face_normal);
+    ov->v.face_shift_code = (uint8_t*)rebase(hv->face_shift_code);
+    ov->v.cell_face_connections = (int32_t*)rebase(hv->cell_face_connections);
+  }
+  mv_context_destroy(ctx);
+  *out = &ov->v;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mv_options_default(mv_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = MV_PRECISION_FILTERED;
+  o->face_mode = MV_FACES_OWNED;
+}
+
+const char* mv_strerror(int s) {
+  switch (s) {
+    case MV_OK: return "ok";
+    case MV_ERR_ARG: return "invalid argument";
+    case MV_ERR_DEGENERATE: return "Degenerate point set! (duplicate generators)";
+    case MV_ERR_RING: return "No suitable vertex found to extend boundary!";
+    case MV_ERR_DET: return "Degenerate 3-plane intersection!";
+    case MV_ERR_CAPACITY: return "a cell exceeded the largest device capacity tier";
+    case MV_ERR_CUDA: return "CUDA runtime error";
+    case MV_ERR_NO_DEVICE: return "no usable CUDA device";
+    case MV_ERR_OOM: return "out of device or pinned host memory";
+    default: return "unknown status";
+  }
+}
+
+const char* mv_version(void) { return "mvgpu 0.1.0 (sm_100a)"; }
+
+int mv_context_create(int device, mv_context** out) {
+  if (!out) return MV_ERR_ARG;
+  *out = nullptr;
+  int dev = device;
+  if (dev < 0) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+      cudaGetLastError();
+      return MV_ERR_NO_DEVICE;
+    }
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || dev >= count) {
+    cudaGetLastError();
+    return MV_ERR_NO_DEVICE;
+  }
+  MV_CUDA(cudaSetDevice(dev));
+  mv_context* ctx = new (std::nothrow) mv_context();
+  if (!ctx) return MV_ERR_OOM;
+  ctx->device = dev;
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return cuda_status(e);
+  }
+  for (int p = 0; p < 2; p++) {
+    ctx->bps_fast[p] = cells_blocks_per_sm_fast(p);
+    ctx->bps_large[p] = cells_blocks_per_sm_large(p);
+  }
+  if (cudaGetLastError() != cudaSuccess || ctx->bps_fast[0] <= 0 || ctx->bps_fast[1] <= 0) {
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return MV_ERR_CUDA;
+  }
+  *out = ctx;
+  return MV_OK;
+}
+
+void mv_context_destroy(mv_context* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs = reinterpret_cast<DevBuf*>(&ctx->ws);
+  const size_t nb = sizeof(Workspace) / sizeof(DevBuf);
+  for (size_t i = 0; i < nb; i++)
+    if (bufs[i].p) cudaFree(bufs[i].p);
+  if (ctx->host) cudaFreeHost(ctx->host);
+  for (int i = 0; i < 8; i++)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int mv_context_last_stats(const mv_context* ctx, mv_build_stats* out) {
+  if (!ctx || !out) return MV_ERR_ARG;
+  *out = ctx->last;
+  return MV_OK;
+}
+
+int mv_context_build_device(mv_context* ctx, const double* d_generators, const uint8_t* d_mask,
+                            int64_t n, const double anchor[3], const double width[3],
+                            int dimensionality, int periodic, const mv_options* opts,
+                            mv_device_voronoi* out) {
+  if (!ctx || !anchor || !width) return MV_ERR_ARG;
+  return build_device_impl(ctx, d_generators, d_mask, n, anchor, width, dimensionality, periodic,
+                           opts, out);
+}
+
+int mv_context_build(mv_context* ctx, const double* generators, const uint8_t* mask, int64_t n,
+                     const double anchor[3], const double width[3], int dimensionality,
+                     int periodic, const mv_options* opts, mv_voronoi** out) {
+  if (!anchor || !width) return MV_ERR_ARG;
+  return build_host_impl(ctx, generators, mask, n, anchor, width, dimensionality, periodic, opts,
+                         out);
+}
+
+int mv_voronoi_build(const double* generators, int64_t n, const double anchor[3],
+                     const double width[3], int dimensionality, int periodic,
+                     const mv_options* opts, mv_voronoi** out) {
+  if (!anchor || !width) return MV_ERR_ARG;
+  return standalone(generators, nullptr, n, anchor, width, dimensionality, periodic, opts, out);
+}
+
+int mv_voronoi_build_partial(const double* generators, const uint8_t* mask, int64_t n,
+                             const double anchor[3], const double width[3], int dimensionality,
+                             int periodic, const mv_options* opts, mv_voronoi** out) {
+  if (!anchor || !width || (n > 0 && !mask)) return MV_ERR_ARG;
+  return standalone(generators, mask, n, anchor, width, dimensionality, periodic, opts, out);
+}
+
+void mv_voronoi_free(mv_voronoi* v) {
+  if (!v || !v->_owner) return;
+  OwnedVoronoi* ov = static_cast<OwnedVoronoi*>(v->_owner);
+  std::free(ov->block);
+  delete ov;
+}
+
+void mv_shift_from_code(int code, const double width[3], double out[3]) {
+  D3 s = shift_of_code(code, width);
+  out[0] = s.x, out[1] = s.y, out[2] = s.z;
+}
+
+}  // extern "C"

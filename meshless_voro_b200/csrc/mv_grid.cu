@@ -1,0 +1,313 @@
+// mv_grid.cu -- uniform grid (neighbour search), prefix sums, face ordering and the
+// cell -> face CSR.
+//
+// Replaces RTree::bulk_load (rtree_nn.rs:6-8) with a device counting sort of the
+// generators into a row-major uniform grid (SoA positions, coalesced for the shell
+// gather of the cell kernel), and the serial flatten + Voronoi::finalize
+// (voronoi.rs:226, 241-263) with scans and scatters.
+#include <cstdint>
+
+#include "mv_internal.h"
+
+namespace mv {
+
+// ------------------------------------------------------------ preparation --
+// Generator::new (generator.rs:13-24): zero the unused coordinates.  Also records the
+// extent of the generators and flags non-finite coordinates.
+__device__ __forceinline__ unsigned long long ord_key(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_val(unsigned long long k) {
+  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+__global__ void prep_kernel(const double* __restrict__ xyz, int n, int dim, double* __restrict__ gen,
+                            unsigned long long* ext_keys /* [6]: min x,y,z, -max x,y,z */,
+                            int* bad) {
+  __shared__ unsigned long long smin[3], smax[3];
+  if (threadIdx.x < 3) {
+    smin[threadIdx.x] = ~0ull;
+    smax[threadIdx.x] = 0ull;
+  }
+  __syncthreads();
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    double c[3] = {xyz[3 * (int64_t)k], xyz[3 * (int64_t)k + 1], xyz[3 * (int64_t)k + 2]};
+    if (dim == 1) c[1] = 0.0, c[2] = 0.0;
+    if (dim == 2) c[2] = 0.0;
+    bool fin = true;
+    for (int i = 0; i < 3; i++) {
+      gen[3 * (int64_t)k + i] = c[i];
+      fin &= isfinite(c[i]);
+    }
+    if (!fin) atomicExch(bad, 1);
+    for (int i = 0; i < 3; i++) {
+      atomicMin(&smin[i], ord_key(c[i]));
+      atomicMax(&smax[i], ord_key(c[i]));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    atomicMin(&ext_keys[threadIdx.x], smin[threadIdx.x]);
+    atomicMax(&ext_keys[3 + threadIdx.x], smax[threadIdx.x]);
+  }
+}
+
+__global__ void ext_finish_kernel(const unsigned long long* ext_keys, double* ext) {
+  int i = threadIdx.x;
+  if (i < 6) ext[i] = ord_val(ext_keys[i]);
+}
+
+struct GridParams {
+  int G[3];
+  double a[3], inv[3];
+};
+
+__global__ void cell_index_kernel(const double* __restrict__ gen, int n, GridParams gp,
+                                  int32_t* __restrict__ cid, int32_t* __restrict__ count) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int c[3];
+  for (int i = 0; i < 3; i++) {
+    double f = floor((gen[3 * (int64_t)k + i] - gp.a[i]) * gp.inv[i]);
+    if (!(f >= 0.0)) f = 0.0;
+    if (f > gp.G[i] - 1) f = gp.G[i] - 1;
+    c[i] = (int)f;
+  }
+  int id = c[0] + gp.G[0] * (c[1] + gp.G[1] * c[2]);
+  cid[k] = id;
+  atomicAdd(count + id, 1);
+}
+
+__global__ void scatter_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ cid,
+                               const int32_t* __restrict__ start, int32_t* __restrict__ fill,
+                               double* __restrict__ sx, double* __restrict__ sy,
+                               double* __restrict__ sz, int32_t* __restrict__ sid) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int c = cid[k];
+  int pos = start[c] + atomicAdd(fill + c, 1);
+  sx[pos] = gen[3 * (int64_t)k];
+  sy[pos] = gen[3 * (int64_t)k + 1];
+  sz[pos] = gen[3 * (int64_t)k + 2];
+  sid[pos] = k;
+}
+
+// ------------------------------------------------------------------- scans --
+// Exclusive scan of int32 counts into int64 offsets, out[n] = total.
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 16;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ long long block_excl_scan(long long v, long long* total) {
+  __shared__ long long wsum[SCAN_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long s = lane < SCAN_THREADS / 32 ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < SCAN_THREADS / 32) wsum[lane] = s;
+  }
+  __syncthreads();
+  long long wpre = w > 0 ? wsum[w - 1] : 0;
+  *total = wsum[SCAN_THREADS / 32 - 1];
+  __syncthreads();
+  return wpre + x - v;
+}
+
+template <class In>
+__global__ void scan_reduce_kernel(const In* __restrict__ in, int64_t n, long long* __restrict__ sums) {
+  int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  long long s = 0;
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int64_t k = base + (int64_t)i * SCAN_THREADS + threadIdx.x;
+    if (k < n) s += (long long)in[k];
+  }
+  long long tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void scan_sums_kernel(long long* sums, int nb) {
+  long long carry = 0;
+  for (int base = 0; base < nb; base += SCAN_THREADS) {
+    int k = base + threadIdx.x;
+    long long v = k < nb ? sums[k] : 0;
+    long long tot;
+    long long ex = block_excl_scan(v, &tot);
+    if (k < nb) sums[k] = carry + ex;
+    carry += tot;
+  }
+}
+
+template <class In, class Out>
+__global__ void scan_final_kernel(const In* __restrict__ in, int64_t n, const long long* __restrict__ sums,
+                                  Out* __restrict__ out) {
+  int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  // each thread owns SCAN_ITEMS consecutive items
+  long long v[SCAN_ITEMS];
+  long long s = 0;
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int64_t k = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
+    v[i] = k < n ? (long long)in[k] : 0;
+    s += v[i];
+  }
+  long long tot;
+  long long ex = block_excl_scan(s, &tot) + sums[blockIdx.x];
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int64_t k = base + (int64_t)threadIdx.x * SCAN_ITEMS + i;
+    if (k < n) out[k] = (Out)ex;
+    if (k == n - 1) out[n] = (Out)(ex + v[i]);
+    ex += v[i];
+  }
+}
+
+// --------------------------------------------------------------- faces/CSR --
+
+// staging slot -> final position: faces grouped by left cell in cell order, inside a
+// cell in clipping-plane order (flatten!, voronoi.rs:226)
+__global__ void reorder_faces_kernel(FaceArrays st, int64_t F, const int64_t* __restrict__ stage_off,
+                                     const int64_t* __restrict__ face_off, FaceArrays out) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= F) return;
+  int left = st.left[q];
+  int64_t f = face_off[left] + (q - stage_off[left]);
+  out.left[f] = left;
+  out.right[f] = st.right[q];
+  out.area[f] = st.area[q];
+  for (int i = 0; i < 3; i++) {
+    out.centroid[3 * f + i] = st.centroid[3 * q + i];
+    out.normal[3 * f + i] = st.normal[3 * q + i];
+  }
+  out.code[f] = st.code[q];
+}
+
+// faces linked to their right cell (voronoi.rs:248-250: internal, unshifted faces)
+__global__ void in_count_kernel(const int32_t* __restrict__ right, const uint8_t* __restrict__ code,
+                                int64_t F, int32_t* __restrict__ in_count) {
+  int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  int r = right[f];
+  if (r >= 0 && code[f] == 13) atomicAdd(in_count + r, 1);
+}
+
+__global__ void conn_count_kernel(const int32_t* __restrict__ face_count,
+                                  const int32_t* __restrict__ in_count, int n,
+                                  int32_t* __restrict__ conn_count) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) conn_count[k] = face_count[k] + in_count[k];
+}
+
+// A cell's connections are its incoming faces (all from lower-indexed cells, so with
+// smaller face indices) followed by its own faces in order.
+__global__ void conn_fill_kernel(const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+                                 const uint8_t* __restrict__ code, int64_t F,
+                                 const int64_t* __restrict__ face_off,
+                                 const int64_t* __restrict__ conn_off,
+                                 const int32_t* __restrict__ in_count, int32_t* __restrict__ cursor,
+                                 int32_t* __restrict__ conn) {
+  int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  int l = left[f];
+  conn[conn_off[l] + in_count[l] + (f - face_off[l])] = (int32_t)f;
+  int r = right[f];
+  if (r >= 0 && code[f] == 13) {
+    int slot = atomicAdd(cursor + r, 1);
+    conn[conn_off[r] + slot] = (int32_t)f;
+  }
+}
+
+__global__ void conn_sort_kernel(const int64_t* __restrict__ conn_off,
+                                 const int32_t* __restrict__ in_count, int n,
+                                 int32_t* __restrict__ conn) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int32_t* a = conn + conn_off[k];
+  int m = in_count[k];
+  for (int i = 1; i < m; i++) {
+    int32_t v = a[i];
+    int j = i - 1;
+    while (j >= 0 && a[j] > v) {
+      a[j + 1] = a[j];
+      j--;
+    }
+    a[j + 1] = v;
+  }
+}
+
+// ---------------------------------------------------------------- launchers --
+static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
+                 double* ext, int* bad, cudaStream_t st) {
+  if (n > 0) prep_kernel<<<nblk(n, 256), 256, 0, st>>>(xyz, n, dim, gen, ext_keys, bad);
+  ext_finish_kernel<<<1, 32, 0, st>>>(ext_keys, ext);
+}
+
+void launch_grid(const double* gen, int n, const int G[3], const double a[3], const double inv[3],
+                 int32_t* cid, int32_t* count, int32_t* start, int32_t* fill, double* sx, double* sy,
+                 double* sz, int32_t* sid, long long* scan_tmp, cudaStream_t st);
+
+template <class In, class Out>
+static void scan_impl(const In* in, int64_t n, Out* out, long long* tmp, cudaStream_t st) {
+  if (n <= 0) {
+    cudaMemsetAsync(out, 0, sizeof(Out), st);
+    return;
+  }
+  int nb = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
+  scan_reduce_kernel<In><<<nb, SCAN_THREADS, 0, st>>>(in, n, tmp);
+  scan_sums_kernel<<<1, SCAN_THREADS, 0, st>>>(tmp, nb);
+  scan_final_kernel<In, Out><<<nb, SCAN_THREADS, 0, st>>>(in, n, tmp, out);
+}
+
+size_t scan_tmp_elems(int64_t n) { return (size_t)((n + SCAN_TILE - 1) / SCAN_TILE) + 1; }
+
+void scan_i32_to_i32(const int32_t* in, int64_t n, int32_t* out, long long* tmp, cudaStream_t st) {
+  scan_impl<int32_t, int32_t>(in, n, out, tmp, st);
+}
+void scan_i32_to_i64(const int32_t* in, int64_t n, int64_t* out, long long* tmp, cudaStream_t st) {
+  scan_impl<int32_t, int64_t>(in, n, out, tmp, st);
+}
+
+void launch_grid(const double* gen, int n, const int G[3], const double a[3], const double inv[3],
+                 int32_t* cid, int32_t* count, int32_t* start, int32_t* fill, double* sx, double* sy,
+                 double* sz, int32_t* sid, long long* scan_tmp, cudaStream_t st) {
+  GridParams gp;
+  for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
+  int64_t ncell = (int64_t)G[0] * G[1] * G[2];
+  if (n > 0) cell_index_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, count);
+  scan_i32_to_i32(count, ncell, start, scan_tmp, st);
+  if (n > 0) scatter_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, cid, start, fill, sx, sy, sz, sid);
+}
+
+void launch_reorder(const FaceArrays& stage, int64_t F, const int64_t* stage_off,
+                    const int64_t* face_off, const FaceArrays& out, cudaStream_t st) {
+  if (F > 0) reorder_faces_kernel<<<nblk(F, 256), 256, 0, st>>>(stage, F, stage_off, face_off, out);
+}
+
+void launch_csr_counts(const FaceArrays& f, int64_t F, const int32_t* face_count, int n,
+                       int32_t* in_count, int32_t* conn_count, cudaStream_t st) {
+  if (F > 0) in_count_kernel<<<nblk(F, 256), 256, 0, st>>>(f.right, f.code, F, in_count);
+  if (n > 0) conn_count_kernel<<<nblk(n, 256), 256, 0, st>>>(face_count, in_count, n, conn_count);
+}
+
+void launch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, const int64_t* conn_off,
+                     const int32_t* in_count, int32_t* cursor, int n, int32_t* conn, cudaStream_t st) {
+  if (F > 0)
+    conn_fill_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, F, face_off, conn_off,
+                                                   in_count, cursor, conn);
+  if (n > 0) conn_sort_kernel<<<nblk(n, 256), 256, 0, st>>>(conn_off, in_count, n, conn);
+}
+
+}  // namespace mv

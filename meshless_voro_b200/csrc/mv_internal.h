@@ -1,0 +1,103 @@
+// mv_internal.h -- structures shared by the kernels and the host orchestration.
+#pragma once
+#include <cstdint>
+
+namespace mv {
+
+// Per-build counters, accumulated on the device (see mv_build_stats in mvgpu.h).
+enum StatSlot {
+  ST_CELLS = 0,
+  ST_NEIGHBOURS,
+  ST_PLANES,
+  ST_F32_UNDECIDED,
+  ST_EXACT,
+  ST_SHELLS,
+  ST_OVERFLOW,
+  ST_SERIAL_RING,
+  ST_COUNT
+};
+
+// Device status words: [0] status code (first error wins), [1] failing cell (min),
+// [2] set when the face staging buffer was too small (the host grows it and reruns).
+enum { STATUS_CODE = 0, STATUS_CELL = 1, STATUS_FACE_OVERFLOW = 2, STATUS_WORDS = 4 };
+
+// Device counters of one build (one allocation, cleared before each build).
+struct DevCounters {
+  unsigned long long face_counter;
+  unsigned long long stats[ST_COUNT];
+  unsigned long long ext_keys[6];
+  double ext[6];
+  int32_t status[STATUS_WORDS];
+  unsigned int work[4];       // work queues of the capacity tiers
+  unsigned int ovf_count[4];  // overflow lists of the capacity tiers
+  int32_t bad_input;
+  int32_t pad[3];
+};
+
+// Face arrays (SoA; centroid and normal are [F][3]).
+struct FaceArrays {
+  int32_t* left;
+  int32_t* right;
+  double* area;
+  double* centroid;
+  double* normal;
+  uint8_t* code;
+};
+
+// One tessellation, as seen by the cell kernel.
+struct Job {
+  // ---- generators ----
+  const double* gen;        // [n][3] by original index, unused dims zeroed (generator.rs:13-24)
+  const double* sx;         // grid-sorted SoA copies
+  const double* sy;
+  const double* sz;
+  const int32_t* sid;       // sorted position -> original index
+  const int32_t* cell_start;  // grid cell -> first sorted position, [ncell + 1]
+  const uint8_t* mask;      // by original index, or nullptr (full build)
+  int32_t n;
+  int32_t dim;
+  int32_t periodic;
+  int32_t face_mode;        // MV_FACES_OWNED / MV_FACES_ALL
+  int32_t precision;        // MV_PRECISION_*
+  // ---- uniform grid ----
+  int32_t G[3];
+  double ga[3];             // grid anchor == normalised simulation anchor
+  double gw[3];             // normalised simulation width (period of the images)
+  double gh[3];             // cell size
+  double ginv[3];           // 1 / cell size
+  const double* ext;        // device [6]: min x,y,z, max x,y,z of the generators
+  double geps[3];           // cell-box inflation against rounding of the cell index
+  double R0;                // first neighbour-shell radius
+  // ---- simulation boundary (boundary.rs:14-47) ----
+  double bn[6][3];
+  double bp[6][3];
+  double bd[6];
+  double iloc_a[3];         // anchor - width of the (tripled) box
+  double iloc_inv[3];       // 1 / (3 width)
+  double xabs_max;          // max |coordinate| over generators (filter bound)
+  // ---- outputs, by original index ----
+  double* volume;
+  double* centroid;         // [n][3]
+  double* safety_radius;
+  int32_t* face_count;      // faces emitted by the cell
+  int64_t* stage_off;       // first staging slot of the cell's faces
+  // ---- face staging (cells append in completion order) ----
+  int32_t* f_left;
+  int32_t* f_right;
+  double* f_area;
+  double* f_centroid;       // [cap][3]
+  double* f_normal;         // [cap][3]
+  uint8_t* f_code;
+  unsigned long long* face_counter;
+  int64_t face_cap;
+  // ---- work distribution / retry queue ----
+  int32_t* order;           // sorted positions to process (overflow pass), or nullptr
+  int32_t n_order;          // number of positions to process
+  unsigned int* work_counter;
+  int32_t* ovf_list;        // cells that outgrew this capacity tier
+  unsigned int* ovf_count;
+  int32_t* status;          // [2]
+  unsigned long long* stats;  // [ST_COUNT]
+};
+
+}  // namespace mv

@@ -1,0 +1,457 @@
+"""Host-side mirror of the meshless_voronoi 0.7.2 public API over the CUDA library.
+
+Same names, argument meaning and error behaviour as the Rust crate:
+``Voronoi.build`` (voronoi.rs:151-159), ``Voronoi.build_partial`` (voronoi.rs:181-190),
+``VoronoiCell`` (voronoi_cell.rs:107-165), ``VoronoiFace`` (voronoi_face.rs:72-131),
+``VoronoiIntegrator`` (voronoi.rs:527-828) with the built-in integrals of
+integrals.rs.  Where the crate panics the library returns a status code and this
+module raises ``MvError``.
+
+Every build runs on the GPU through libmvgpu.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass
+from typing import Iterator, Optional
+
+import numpy as np
+
+from . import _native as N
+
+
+class Dimensionality(enum.IntEnum):
+    """voronoi.rs:31-40"""
+    OneD = 1
+    TwoD = 2
+    ThreeD = 3
+
+    def vector_is_valid(self, v) -> bool:
+        """voronoi.rs:42-49"""
+        if self == Dimensionality.OneD:
+            return v[1] == 0.0 and v[2] == 0.0
+        if self == Dimensionality.TwoD:
+            return v[2] == 0.0
+        return True
+
+
+PRECISION = {"fp64": N.MV_PRECISION_FP64, "filtered": N.MV_PRECISION_FILTERED}
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _vec3(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(3))
+
+
+def shift_from_code(code: int, width) -> Optional[np.ndarray]:
+    """The reference's Option<DVec3> shift for a face shift code (rtree_nn.rs:27-33)."""
+    if code == N.NO_SHIFT:
+        return None
+    out = np.zeros(3)
+    N.lib().mv_shift_from_code(int(code), _dp(_vec3(width)), _dp(out))
+    return out
+
+
+def make_options(precision="filtered", face_mode=N.MV_FACES_OWNED, stream=None,
+                 points_per_grid_cell=0.0, initial_radius=0.0) -> N.Options:
+    o = N.Options()
+    N.lib().mv_options_default(C.byref(o))
+    o.precision = PRECISION[precision] if isinstance(precision, str) else int(precision)
+    o.face_mode = int(face_mode)
+    o.points_per_grid_cell = float(points_per_grid_cell)
+    o.initial_radius = float(initial_radius)
+    o.stream = stream
+    return o
+
+
+class Context:
+    """A device, its CUDA stream and the reusable device workspace (mv_context)."""
+
+    def __init__(self, device: int = -1):
+        h = C.c_void_p()
+        N.check(N.lib().mv_context_create(int(device), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            N.lib().mv_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_stats(self) -> dict:
+        s = N.BuildStats()
+        N.check(N.lib().mv_context_last_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def build_arrays(self, generators, mask, anchor, width, dimensionality, periodic,
+                     precision="filtered", face_mode=N.MV_FACES_OWNED, **kw) -> "VoronoiArrays":
+        """Host arrays in, host arrays out (mv_context_build); results are copied."""
+        g = np.ascontiguousarray(np.asarray(generators, dtype=np.float64).reshape(-1, 3))
+        n = g.shape[0]
+        m = None
+        if mask is not None:
+            m = np.ascontiguousarray(np.asarray(mask, dtype=np.bool_).reshape(n)).view(np.uint8)
+        a, w = _vec3(anchor), _vec3(width)
+        opts = make_options(precision, face_mode, **kw)
+        out = C.POINTER(N.HostVoronoi)()
+        rc = N.lib().mv_context_build(self._h, g.ctypes.data_as(C.c_void_p),
+                                      m.ctypes.data_as(C.c_void_p) if m is not None else None,
+                                      n, _dp(a), _dp(w), int(dimensionality), int(bool(periodic)),
+                                      C.byref(opts), C.byref(out))
+        if rc != N.MV_OK:
+            cell = out.contents.error_cell if out else -1
+            raise N.MvError(rc, cell)
+        return VoronoiArrays.from_host(out.contents, g, m, copy=True)
+
+    def build_device(self, d_generators: int, d_mask: int, n: int, anchor, width,
+                     dimensionality, periodic, precision="filtered",
+                     face_mode=N.MV_FACES_OWNED, stream=None, **kw) -> N.DeviceVoronoi:
+        """Device pointers in, device pointers (owned by this context) out."""
+        a, w = _vec3(anchor), _vec3(width)
+        opts = make_options(precision, face_mode, stream=stream, **kw)
+        out = N.DeviceVoronoi()
+        rc = N.lib().mv_context_build_device(self._h, C.c_void_p(d_generators),
+                                             C.c_void_p(d_mask) if d_mask else None, int(n),
+                                             _dp(a), _dp(w), int(dimensionality),
+                                             int(bool(periodic)), C.byref(opts), C.byref(out))
+        if rc != N.MV_OK:
+            raise N.MvError(rc, out.error_cell)
+        return out
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(-1)
+    return _default_ctx
+
+
+@dataclass
+class VoronoiArrays:
+    """Flat, reference-ordered results of one build (numpy, host)."""
+    n_cells: int
+    anchor: np.ndarray
+    width: np.ndarray
+    dimensionality: int
+    periodic: bool
+    cell_volume: np.ndarray
+    cell_centroid: np.ndarray
+    cell_loc: np.ndarray
+    cell_safety_radius: np.ndarray
+    cell_face_offset: Optional[np.ndarray]
+    cell_face_count: Optional[np.ndarray]
+    face_left: np.ndarray
+    face_right: np.ndarray
+    face_area: np.ndarray
+    face_centroid: np.ndarray
+    face_normal: np.ndarray
+    face_shift_code: np.ndarray
+    cell_face_connections: Optional[np.ndarray]
+
+    @staticmethod
+    def from_host(hv: N.HostVoronoi, generators: np.ndarray, mask_u8, copy=True) -> "VoronoiArrays":
+        n, F, Cn = int(hv.n_cells), int(hv.n_faces), int(hv.n_connections)
+
+        def arr(ptr, count, dtype, shape=None):
+            if count == 0 or not ptr:
+                a = np.zeros(0 if shape is None else (0,) + shape[1:], dtype=dtype)
+                return a
+            a = np.ctypeslib.as_array(ptr, shape=(count,))
+            a = a.astype(dtype, copy=True) if copy else a
+            return a.reshape(shape) if shape else a
+
+        dim = int(hv.dimensionality)
+        loc = generators.copy()
+        if dim == 1:
+            loc[:, 1:] = 0.0
+        elif dim == 2:
+            loc[:, 2] = 0.0
+        if mask_u8 is not None:
+            loc[mask_u8 == 0] = 0.0
+        has_csr = bool(hv.cell_face_offset)
+        return VoronoiArrays(
+            n_cells=n, anchor=np.array(hv.anchor[:]), width=np.array(hv.width[:]),
+            dimensionality=dim, periodic=bool(hv.periodic),
+            cell_volume=arr(hv.cell_volume, n, np.float64),
+            cell_centroid=arr(hv.cell_centroid, 3 * n, np.float64, (n, 3)),
+            cell_loc=loc,
+            cell_safety_radius=arr(hv.cell_safety_radius, n, np.float64),
+            cell_face_offset=arr(hv.cell_face_offset, n, np.int64) if has_csr else None,
+            cell_face_count=arr(hv.cell_face_count, n, np.int64) if has_csr else None,
+            face_left=arr(hv.face_left, F, np.int64),
+            face_right=arr(hv.face_right, F, np.int64),
+            face_area=arr(hv.face_area, F, np.float64),
+            face_centroid=arr(hv.face_centroid, 3 * F, np.float64, (F, 3)),
+            face_normal=arr(hv.face_normal, 3 * F, np.float64, (F, 3)),
+            face_shift_code=arr(hv.face_shift_code, F, np.int32),
+            cell_face_connections=arr(hv.cell_face_connections, Cn, np.int64) if has_csr else None,
+        )
+
+
+class VoronoiCell:
+    """voronoi_cell.rs:11-165 (a view into a Voronoi)."""
+
+    __slots__ = ("_v", "_i")
+
+    def __init__(self, voronoi: "Voronoi", idx: int):
+        self._v = voronoi
+        self._i = idx
+
+    def loc(self) -> np.ndarray:
+        return self._v.arrays.cell_loc[self._i]
+
+    def centroid(self) -> np.ndarray:
+        return self._v.arrays.cell_centroid[self._i]
+
+    def volume(self) -> float:
+        return float(self._v.arrays.cell_volume[self._i])
+
+    def safety_radius(self) -> float:
+        return float(self._v.arrays.cell_safety_radius[self._i])
+
+    def face_connections_offset(self) -> int:
+        return int(self._v.arrays.cell_face_offset[self._i])
+
+    def face_count(self) -> int:
+        return int(self._v.arrays.cell_face_count[self._i])
+
+    def face_indices(self, voronoi: "Voronoi" = None) -> np.ndarray:
+        v = voronoi or self._v
+        o = self.face_connections_offset()
+        return v.arrays.cell_face_connections[o:o + self.face_count()]
+
+    def faces(self, voronoi: "Voronoi" = None) -> Iterator["VoronoiFace"]:
+        v = voronoi or self._v
+        for f in self.face_indices(v):
+            yield VoronoiFace(v, int(f))
+
+    def neighbour_ids(self, voronoi: "Voronoi" = None) -> Iterator[int]:
+        """voronoi_cell.rs:141-153: other side of every non-periodic, non-boundary face.
+        An inactive cell has index 0 in the reference (VoronoiCell::default)."""
+        v = voronoi or self._v
+        a = v.arrays
+        my_idx = self._i if a.cell_volume[self._i] != 0.0 or not v._partial else 0
+        for f in self.face_indices(v):
+            if a.face_shift_code[f] != N.NO_SHIFT or a.face_right[f] < 0:
+                continue
+            yield int(a.face_right[f]) if a.face_left[f] == my_idx else int(a.face_left[f])
+
+
+class VoronoiFace:
+    """voronoi_face.rs:48-132 (a view into a Voronoi)."""
+
+    __slots__ = ("_v", "_f")
+
+    def __init__(self, voronoi: "Voronoi", idx: int):
+        self._v = voronoi
+        self._f = idx
+
+    def left(self) -> int:
+        return int(self._v.arrays.face_left[self._f])
+
+    def right(self) -> Optional[int]:
+        r = int(self._v.arrays.face_right[self._f])
+        return None if r < 0 else r
+
+    def area(self) -> float:
+        return float(self._v.arrays.face_area[self._f])
+
+    def centroid(self) -> np.ndarray:
+        return self._v.arrays.face_centroid[self._f]
+
+    def normal(self) -> np.ndarray:
+        return self._v.arrays.face_normal[self._f]
+
+    def shift(self) -> Optional[np.ndarray]:
+        return shift_from_code(int(self._v.arrays.face_shift_code[self._f]), self._v.width())
+
+    def is_periodic(self) -> bool:
+        return int(self._v.arrays.face_shift_code[self._f]) != N.NO_SHIFT
+
+    def is_boundary(self) -> bool:
+        return int(self._v.arrays.face_right[self._f]) < 0
+
+
+class Voronoi:
+    """voronoi.rs:110-408"""
+
+    def __init__(self, arrays: VoronoiArrays, partial: bool = False):
+        self.arrays = arrays
+        self._partial = partial
+
+    @staticmethod
+    def build(generators, anchor, width, dimensionality=Dimensionality.ThreeD, periodic=False, *,
+              precision="filtered", context: Context = None, **kw) -> "Voronoi":
+        ctx = context or default_context()
+        a = ctx.build_arrays(generators, None, anchor, width, int(dimensionality), periodic,
+                             precision=precision, **kw)
+        return Voronoi(a)
+
+    @staticmethod
+    def build_partial(generators, mask, anchor, width, dimensionality=Dimensionality.ThreeD,
+                      periodic=False, *, precision="filtered", context: Context = None,
+                      **kw) -> "Voronoi":
+        ctx = context or default_context()
+        a = ctx.build_arrays(generators, mask, anchor, width, int(dimensionality), periodic,
+                             precision=precision, **kw)
+        return Voronoi(a, partial=True)
+
+    def anchor(self) -> np.ndarray:
+        return self.arrays.anchor
+
+    def width(self) -> np.ndarray:
+        return self.arrays.width
+
+    def cells(self):
+        return [VoronoiCell(self, i) for i in range(self.arrays.n_cells)]
+
+    def faces(self):
+        return [VoronoiFace(self, f) for f in range(len(self.arrays.face_left))]
+
+    def cell_face_connections(self) -> np.ndarray:
+        return self.arrays.cell_face_connections
+
+    def dimensionality(self) -> int:
+        return self.arrays.dimensionality
+
+    def periodic(self) -> bool:
+        return self.arrays.periodic
+
+
+# ------------------------------------------------------------ integrals.rs --
+class VolumeIntegral:
+    """integrals.rs:124-142"""
+    __slots__ = ("volume",)
+
+    def __init__(self, volume):
+        self.volume = volume
+
+
+class VolumeCentroidIntegral:
+    """integrals.rs:69-106"""
+    __slots__ = ("volume", "centroid")
+
+    def __init__(self, volume, centroid):
+        self.volume = volume
+        self.centroid = centroid
+
+
+class AreaIntegral:
+    """integrals.rs:343-361"""
+    __slots__ = ("area",)
+
+    def __init__(self, area, centroid=None):
+        self.area = area
+
+
+class AreaCentroidIntegral:
+    """integrals.rs:283-320"""
+    __slots__ = ("area", "centroid")
+
+    def __init__(self, area, centroid):
+        self.area = area
+        self.centroid = centroid
+
+
+class FaceIntegrator:
+    """integrals.rs:204-259"""
+    __slots__ = ("_left", "_right", "_shift", "_integral")
+
+    def __init__(self, left, right, shift, integral):
+        self._left, self._right, self._shift, self._integral = left, right, shift, integral
+
+    def left(self):
+        return self._left
+
+    def right(self):
+        return self._right
+
+    def shift(self):
+        return self._shift
+
+    def integral(self):
+        return self._integral
+
+
+class VoronoiIntegrator:
+    """voronoi.rs:527-828 with the crate's built-in integrals evaluated on the GPU."""
+
+    def __init__(self, generators, mask, anchor, width, dimensionality, periodic, precision,
+                 context):
+        self._g = np.ascontiguousarray(np.asarray(generators, dtype=np.float64).reshape(-1, 3))
+        self._mask = None if mask is None else np.asarray(mask, dtype=bool).reshape(-1)
+        self._anchor, self._width = _vec3(anchor), _vec3(width)
+        self._dim = int(dimensionality)
+        self._periodic = bool(periodic)
+        self._precision = precision
+        self._ctx = context or default_context()
+        self._cache = {}
+
+    @staticmethod
+    def build(generators, mask, anchor, width, dimensionality=Dimensionality.ThreeD,
+              periodic=False, *, precision="filtered", context: Context = None):
+        return VoronoiIntegrator(generators, mask, anchor, width, dimensionality, periodic,
+                                 precision, context)
+
+    def _run(self, face_mode) -> VoronoiArrays:
+        if face_mode not in self._cache:
+            self._cache[face_mode] = self._ctx.build_arrays(
+                self._g, self._mask, self._anchor, self._width, self._dim, self._periodic,
+                precision=self._precision, face_mode=face_mode)
+        return self._cache[face_mode]
+
+    def _active(self):
+        n = self._g.shape[0]
+        return np.ones(n, dtype=bool) if self._mask is None else self._mask
+
+    def compute_cell_integrals(self, integral=VolumeCentroidIntegral):
+        """voronoi.rs:668-673: one integral per active cell, in cell order."""
+        a = self._run(N.MV_FACES_OWNED)
+        idx = np.nonzero(self._active())[0]
+        if integral is VolumeIntegral:
+            return [VolumeIntegral(float(a.cell_volume[i])) for i in idx]
+        if integral is VolumeCentroidIntegral:
+            return [VolumeCentroidIntegral(float(a.cell_volume[i]), a.cell_centroid[i]) for i in idx]
+        raise NotImplementedError("custom cell integrals are not available on the device")
+
+    def _faces(self, a: VoronoiArrays, integral):
+        out = []
+        for f in range(len(a.face_left)):
+            r = int(a.face_right[f])
+            shift = shift_from_code(int(a.face_shift_code[f]), a.width)
+            if integral is AreaIntegral:
+                val = AreaIntegral(float(a.face_area[f]))
+            elif integral is AreaCentroidIntegral:
+                val = AreaCentroidIntegral(float(a.face_area[f]), a.face_centroid[f])
+            else:
+                raise NotImplementedError("custom face integrals are not available on the device")
+            out.append(FaceIntegrator(int(a.face_left[f]), None if r < 0 else r, shift, val))
+        return out
+
+    def compute_face_integrals(self, integral=AreaCentroidIntegral):
+        """voronoi.rs:709-714: every face of every active cell (non-symmetric)."""
+        return self._faces(self._run(N.MV_FACES_ALL), integral)
+
+    def compute_face_integrals_sym(self, integral=AreaCentroidIntegral):
+        """voronoi.rs:725-732: each face once."""
+        return self._faces(self._run(N.MV_FACES_OWNED), integral)
+
+    def to_voronoi(self) -> Voronoi:
+        """From<&VoronoiIntegrator> for Voronoi (voronoi.rs:494-513)."""
+        return Voronoi(self._run(N.MV_FACES_OWNED), partial=self._mask is not None)

@@ -1,0 +1,63 @@
+"""Seeded synthetic generator sets with the shapes of the benchmark configurations.
+
+No public dataset is involved; every set is drawn from numpy's PCG64 with a fixed
+seed so tests, the benchmark and the CPU baseline see identical inputs.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def perturbed_grid(anchor, width, count, pert, rng):
+    """count^3 lattice points (i + 0.5 + pert * U(-0.5, 0.5)) * width / count + anchor,
+    clamped to the box -- the recipe of the reference's perturbed_grid test helper
+    (voronoi.rs:840-859) with a seeded generator."""
+    anchor = np.asarray(anchor, dtype=np.float64)
+    width = np.asarray(width, dtype=np.float64)
+    n = np.arange(count ** 3)
+    idx = np.stack([n // count ** 2, (n % count ** 2) // count, n % count], axis=1).astype(np.float64)
+    jit = rng.uniform(-0.5, 0.5, size=idx.shape) if pert != 0 else 0.0
+    pos = (idx + 0.5 + pert * jit) * width / count + anchor
+    return np.clip(pos, anchor, anchor + width)
+
+
+def perturbed_plane(anchor, width, count, pert, rng):
+    """count^2 points in the z = anchor.z + width.z / 2 plane (voronoi.rs:882-900)."""
+    anchor = np.asarray(anchor, dtype=np.float64)
+    width = np.asarray(width, dtype=np.float64)
+    n = np.arange(count ** 2)
+    i, j = (n // count).astype(np.float64), (n % count).astype(np.float64)
+    jit = rng.uniform(-0.5, 0.5, size=(count ** 2, 2)) if pert != 0 else np.zeros((count ** 2, 2))
+    pos = np.stack([i + 0.5 + pert * jit[:, 0], j + 0.5 + pert * jit[:, 1],
+                    np.full(count ** 2, 0.5 * count)], axis=1) * width / count + anchor
+    return np.clip(pos, anchor, anchor + width)
+
+
+def jittered_lattice_32(seed=1):
+    """32^3 lattice of spacing 1/32 in [0,1]^3, U(+-0.25 spacing) jitter, rectangular."""
+    rng = np.random.default_rng(seed)
+    g = perturbed_grid([0, 0, 0], [1, 1, 1], 32, 0.5, rng)
+    return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=3,
+                periodic=False, name="jittered_lattice_32^3_rect")
+
+
+def exact_lattice(count=64):
+    """count^3 unperturbed lattice (i + 0.5) / count, periodic unit box."""
+    g = perturbed_grid([0, 0, 0], [1, 1, 1], count, 0.0, None)
+    return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=3,
+                periodic=True, name=f"exact_lattice_{count}^3_periodic")
+
+
+def poisson(n, seed=3, periodic=True, dim=3):
+    """n i.i.d. uniform points in the unit box."""
+    rng = np.random.default_rng(seed)
+    g = rng.uniform(0.0, 1.0, size=(n, 3))
+    if dim < 3:
+        g[:, dim:] = 0.0
+    return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=dim,
+                periodic=periodic, name=f"poisson_{n}_{'periodic' if periodic else 'rect'}")
+
+
+def poisson_256(seed=3):
+    """256^3 = 16,777,216 i.i.d. uniform points in [0,1)^3, periodic (the headline)."""
+    return poisson(256 ** 3, seed=seed, periodic=True)

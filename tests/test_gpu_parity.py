@@ -1,0 +1,175 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Topology -- faces (left, right, shift), their order, and the cell -> face CSR -- must
+be identical.  Floating-point outputs must agree within 1e-12 relative to the
+cell's scale; since the kernel keeps the reference's operation order they are
+expected to be bit-identical, which is checked separately.
+"""
+import json
+import math
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+import meshless_voro_b200 as mv
+from meshless_voro_b200 import workloads as W
+from meshless_voro_b200._native import MV_FACES_ALL, MV_FACES_OWNED, MvError
+from voronoi_checks import consistency_check
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+REL_TOL = 1e-12
+
+
+def _case(name):
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    if name == "single":
+        return dict(generators=[[0.5, 0.5, 0.5]], anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=False)
+    if name == "two":
+        return dict(generators=[[0.3, 0.4, 0.25], [0.7, 0.6, 0.75]], anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=False)
+    if name == "five_2d":
+        d = math.sqrt(0.1)
+        g = [[0.5, 0.5, 0.5], [0.5 - d, 0.5 - d, 0.5], [0.5 - d, 0.5 + d, 0.5], [0.5 + d, 0.5 + d, 0.5], [0.5 + d, 0.5 - d, 0.5]]
+        return dict(generators=g, anchor=[0, 0, 0], width=[1, 1, 1], dim=2, periodic=False)
+    if name == "four_2d_periodic":
+        g = [[0.4, 0.3, 0], [1.6, 0.2, 0], [0.6, 0.8, 0], [1.4, 0.7, 0]]
+        return dict(generators=g, anchor=[0, 0, 0], width=[2, 1, 1], dim=2, periodic=True)
+    if name == "lattice4_rect":
+        return dict(generators=W.perturbed_grid([0, 0, 0], [1, 1, 1], 4, 0.0, None), anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=False)
+    if name == "lattice12_periodic":
+        return dict(generators=W.perturbed_grid([0, 0, 0], [1, 1, 1], 12, 0.0, None), anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=True)
+    if name == "jitter16_rect":
+        return dict(generators=W.perturbed_grid([0, 0, 0], [1, 1, 1], 16, 0.5, rng), anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=False)
+    if name == "grid15_w2":
+        return dict(generators=W.perturbed_grid([0, 0, 0], [2, 2, 2], 15, 0.95, rng), anchor=[0, 0, 0], width=[2, 2, 2], dim=3, periodic=False)
+    if name == "poisson20k_periodic":
+        return dict(generators=rng.uniform(0, 1, (20000, 3)), anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=True)
+    if name == "poisson5k_rect_aniso":
+        g = rng.uniform(0, 1, (5000, 3)) * [3.0, 1.0, 0.5] + [-1.0, 2.0, 0.25]
+        return dict(generators=g, anchor=[-1.0, 2.0, 0.25], width=[3.0, 1.0, 0.5], dim=3, periodic=False)
+    if name == "small_periodic_17":
+        return dict(generators=rng.uniform(0, 1, (17, 3)), anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=True)
+    if name == "plane25_periodic_2d":
+        return dict(generators=W.perturbed_plane([2, 2, 2], [2, 2, 1], 25, 0.95, rng), anchor=[2, 2, 2], width=[2, 2, 1], dim=2, periodic=True)
+    if name == "poisson_2d_rect":
+        return dict(generators=rng.uniform(0, 1, (3000, 3)), anchor=[0, 0, 0], width=[1, 1, 1], dim=2, periodic=False)
+    if name == "line_1d_periodic":
+        return dict(generators=rng.uniform(0, 1, (200, 3)), anchor=[0, 0, 0], width=[1, 1, 1], dim=1, periodic=True)
+    if name == "non_perturbed_z":
+        fx = json.load(open(os.path.join(HERE, "golden", "non_perturbed_z.json")))
+        return dict(generators=fx["generators"], anchor=fx["anchor"], width=fx["width"], dim=3, periodic=False)
+    if name == "degenerate_2e15":
+        g = W.perturbed_grid([0, 0, 0], [2e15] * 3, 10, 0.0, None)
+        g[42] = 1e14 * np.array([1.00007490802, 9.00019014286, 5.00014639879])
+        return dict(generators=g, anchor=[0, 0, 0], width=[2e15] * 3, dim=3, periodic=False)
+    raise KeyError(name)
+
+
+CASES = ["single", "two", "five_2d", "four_2d_periodic", "lattice4_rect", "lattice12_periodic",
+         "jitter16_rect", "grid15_w2", "poisson20k_periodic", "poisson5k_rect_aniso",
+         "small_periodic_17", "plane25_periodic_2d", "poisson_2d_rect", "line_1d_periodic",
+         "non_perturbed_z", "degenerate_2e15"]
+
+
+def _rel_err(a, b, scale):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.size == 0:
+        return 0.0
+    return float(np.max(np.abs(a - b) / (np.abs(b) + scale)))
+
+
+def compare(gpu, orc, faces_all=False):
+    """Topology identical, floats within REL_TOL; returns True when bit-identical."""
+    assert orc.status == 0
+    n = len(orc.volume)
+    assert np.array_equal(gpu.face_left, orc.face_left)
+    assert np.array_equal(gpu.face_right, orc.face_right)
+    assert np.array_equal(gpu.face_shift_code, orc.face_shift_code)
+    if not faces_all:
+        assert np.array_equal(gpu.cell_face_offset, orc.face_offset)
+        assert np.array_equal(gpu.cell_face_count, orc.face_count)
+        assert np.array_equal(gpu.cell_face_connections, orc.cell_face_connections)
+    vscale = float(np.max(np.abs(orc.volume))) if n else 1.0
+    lscale = vscale ** (1.0 / 3.0) if vscale > 0 else 1.0
+    assert _rel_err(gpu.cell_volume, orc.volume, 1e-300) <= REL_TOL
+    assert _rel_err(gpu.cell_centroid, orc.centroid, lscale) <= REL_TOL
+    assert _rel_err(gpu.cell_safety_radius, orc.safety_radius, 1e-300) <= REL_TOL
+    ascale = float(np.max(np.abs(orc.face_area))) if len(orc.face_area) else 1.0
+    assert _rel_err(gpu.face_area, orc.face_area, ascale * 1e-6) <= REL_TOL
+    assert _rel_err(gpu.face_centroid, orc.face_centroid, lscale) <= REL_TOL
+    assert np.array_equal(gpu.face_normal, orc.face_normal)
+    return (np.array_equal(gpu.cell_volume, orc.volume)
+            and np.array_equal(gpu.cell_centroid, orc.centroid)
+            and np.array_equal(gpu.face_area, orc.face_area)
+            and np.array_equal(gpu.face_centroid, orc.face_centroid))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "filtered"])
+@pytest.mark.parametrize("name", CASES)
+def test_parity_full_build(gpu_ctx, oracle, name, precision):
+    c = _case(name)
+    orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"], periodic=c["periodic"])
+    gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], c["dim"],
+                               c["periodic"], precision=precision)
+    bit_identical = compare(gpu, orc)
+    assert bit_identical, "expected bit-identical integrals"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "filtered"])
+@pytest.mark.parametrize("name", ["grid15_w2", "poisson20k_periodic", "plane25_periodic_2d"])
+def test_parity_partial(gpu_ctx, oracle, name, precision):
+    c = _case(name)
+    n = len(c["generators"])
+    rng = np.random.default_rng(7)
+    for mask in (rng.uniform(size=n) < 0.25, np.eye(1, n, n // 2, dtype=bool)[0]):
+        orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"],
+                           periodic=c["periodic"], mask=mask)
+        gpu = gpu_ctx.build_arrays(c["generators"], mask, c["anchor"], c["width"], c["dim"],
+                                   c["periodic"], precision=precision)
+        assert compare(gpu, orc)
+        assert np.all(gpu.cell_volume[~mask] == 0.0)
+
+
+@pytest.mark.parametrize("name", ["grid15_w2", "poisson20k_periodic", "plane25_periodic_2d"])
+def test_parity_all_faces_integrator(gpu_ctx, oracle, name):
+    """compute_face_integrals (non-symmetric): every face of every cell."""
+    c = _case(name)
+    orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"],
+                       periodic=c["periodic"], flags=oracle.FACES_ALL | oracle.NO_CSR)
+    gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], c["dim"],
+                               c["periodic"], face_mode=MV_FACES_ALL)
+    assert compare(gpu, orc, faces_all=True)
+
+
+def test_reference_api_kats(gpu_ctx):
+    """The reference's own unit tests, run through the mirrored API on the GPU."""
+    v = mv.Voronoi.build([[0.5, 0.5, 0.5]], [0, 0, 0], [1, 1, 1], mv.Dimensionality.ThreeD, False,
+                         context=gpu_ctx)
+    assert abs(v.cells()[0].volume() - 1.0) < 1e-15
+    for n in (2, 3, 4):
+        g = W.perturbed_grid([0, 0, 0], [1, 1, 1], n, 0.0, None)
+        v = mv.Voronoi.build(g, [0, 0, 0], [1, 1, 1], 3, False, context=gpu_ctx)
+        assert np.allclose(v.arrays.cell_volume, 1.0 / n ** 3, rtol=0, atol=1e-15)
+    g = W.perturbed_grid([0, 0, 0], [2, 2, 2], 15, 0.95, np.random.default_rng(3))
+    v = mv.Voronoi.build(g, [0, 0, 0], [2, 2, 2], 3, False, context=gpu_ctx)
+    a = v.arrays
+    consistency_check(a, 3, [2, 2, 2])
+    # neighbour_ids of a cell are the other side of its internal faces
+    cell = v.cells()[100]
+    ids = sorted(cell.neighbour_ids())
+    assert len(ids) == cell.face_count() - sum(1 for f in cell.faces() if f.is_boundary())
+
+
+def test_duplicate_generators_raise(gpu_ctx):
+    g = [[0.2, 0.2, 0.2], [0.7, 0.7, 0.7], [0.2, 0.2, 0.2]]
+    with pytest.raises(MvError) as e:
+        gpu_ctx.build_arrays(g, None, [0, 0, 0], [1, 1, 1], 3, False)
+    assert e.value.status == 2
+
+
+def test_empty_input(gpu_ctx):
+    a = gpu_ctx.build_arrays(np.zeros((0, 3)), None, [0, 0, 0], [1, 1, 1], 3, False)
+    assert a.n_cells == 0 and len(a.face_left) == 0
