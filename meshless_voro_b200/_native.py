@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libmvgpu.so")
+# MVGPU_LIBRARY selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("MVGPU_LIBRARY") or os.path.join(_HERE, "_lib", "libmvgpu.so")
 
 MV_OK = 0
 MV_ERR_ARG = 1

@@ -30,8 +30,9 @@ namespace mv {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-template <int VMAX_, int PMAX_, int CMAX_, typename PIdx_>
+template <int VMAX_, int PMAX_, int CMAX_, typename PIdx_, int MINB_>
 struct Tier {
+  static constexpr int MINB = MINB_;  // min resident blocks per SM (register budget)
   static constexpr int VMAX = VMAX_;
   static constexpr int PMAX = PMAX_;
   static constexpr int CMAX = CMAX_;
@@ -42,8 +43,12 @@ struct Tier {
   static_assert(PMAX < (int)NONE, "plane index type too small");
 };
 
-using TierFast = Tier<64, 64, 128, uint8_t>;
-using TierLarge = Tier<512, 512, 512, uint16_t>;
+// Resident blocks per SM the fast tier is compiled for (sets its register budget).
+#ifndef MV_FAST_MINB
+#define MV_FAST_MINB 4
+#endif
+using TierFast = Tier<64, 64, 128, uint8_t, MV_FAST_MINB>;
+using TierLarge = Tier<512, 512, 512, uint16_t, 1>;
 
 template <class T>
 struct CellSmem {
@@ -60,6 +65,7 @@ struct CellSmem {
   float fx[T::VMAX], fy[T::VMAX], fz[T::VMAX];  // f32 (v - x) for the filter
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
+  unsigned long long cnt[ST_COUNT];  // per-warp counters (flushed at exit)
   union {
     struct {
       unsigned long long key[T::CMAX];
@@ -167,7 +173,7 @@ __device__ __noinline__ int exact_clip(const Job& J, const CellSmem<T>& S, int v
 
 // Vertex::from_dual (convex_cell.rs:28-48); writes vertex slot `slot`.
 template <class T>
-__device__ __forceinline__ bool make_vertex(CellSmem<T>& S, int slot, int i, int j, int k, D3 x,
+__device__ __noinline__ bool make_vertex(CellSmem<T>& S, int slot, int i, int j, int k, D3 x,
                                             int dim) {
   D3 loc;
   bool ok = intersect3({S.pnx[i], S.pny[i], S.pnz[i]}, S.pd[i], {S.pnx[j], S.pny[j], S.pnz[j]},
@@ -198,10 +204,6 @@ __device__ __forceinline__ double amax_of(double max_r2, int dim) {
 
 enum CellResult { CELL_DONE = 0, CELL_OVERFLOW = 1, CELL_ERROR = 2, CELL_FACE_OVERFLOW = 3 };
 
-struct WarpCounters {
-  unsigned long long c[ST_COUNT];
-};
-
 // ------------------------------------------------------------- neighbour shell --
 // Gathers every stream element (generator, periodic image) with lo2 <= d2 < R*R into
 // S.u.g (unsorted) and returns how many there are (may exceed CMAX).  *exhausted is
@@ -210,7 +212,7 @@ struct WarpCounters {
 // (g - q).length_squared() for nn_iter (rstar) and |(q + s) - g|^2 for
 // wrapping_nn_iter (rtree_nn.rs:138-146).
 template <class T>
-__device__ int gather_shell(const Job& J, CellSmem<T>& S, int lane, D3 x, double R, double lo2,
+__device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane, D3 x, double R, double lo2,
                             const double* ext, bool* exhausted) {
   const double xa[3] = {x.x, x.y, x.z};
   int lo[3], hi[3];
@@ -348,7 +350,7 @@ __device__ int gather_shell(const Job& J, CellSmem<T>& S, int lane, D3 x, double
 
 // Bitonic sort of S.u.g.(key, tie)[0, n) ascending; n <= CMAX, padded to a power of 2.
 template <class T>
-__device__ void sort_shell(CellSmem<T>& S, int lane, int n) {
+__device__ __noinline__ void sort_shell(CellSmem<T>& S, int lane, int n) {
   int np2 = 32;
   while (np2 < n) np2 <<= 1;
   for (int i = n + lane; i < np2; i += 32) {
@@ -382,7 +384,7 @@ __device__ void sort_shell(CellSmem<T>& S, int lane, int n) {
 // (simple_cycle.rs:17-78) on lane 0 for the removed vertices at [nvf, nv).
 // Produces the edge list (S.ea, S.eb) and returns its length, or -1 on failure.
 template <class T>
-__device__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np) {
+__device__ __noinline__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np) {
   using PIdx = typename T::PIdx;
   for (int i = 0; i < np; i++) S.rptr[i] = (PIdx)i;
   auto contains = [&](int i) { return S.rptr[i] != (PIdx)i; };
@@ -447,7 +449,7 @@ __device__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np) {
 // vertex's dual[0] whenever that node is still on the boundary.  Returns the edge
 // count, or -1 when the serial replay must decide.
 template <class T>
-__device__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
+__device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
   using PIdx = typename T::PIdx;
   const int r = nv - nvf;
   for (int q = lane; q < r; q += 32) {
@@ -515,9 +517,162 @@ __device__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
 }
 
 // ------------------------------------------------------------------ the cell --
+// Per-warp counters live in shared memory (lane 0 updates them).
+#define WCNT(S, slot, v) \
+  do {                   \
+    if (lane == 0) (S).cnt[slot] += (unsigned long long)(v); \
+  } while (0)
+
+// Integrals and face emission of a finished cell (convex_cell.rs:131-187,
+// voronoi_cell.rs:40-100).  Tets go through 30-lane steps (5 vertices x 6 tets);
+// lanes 0-3 sum the cell integrals and lane p owns face p (and p + 32k), all in the
+// reference's tet order.
+template <class T>
+__device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lane, int self, D3 x,
+                                           int nv, int np, double sr, int* err_code) {
+  const int dim = J.dim;
+  double cacc = 0.0;  // lanes 0..3: volume, centroid x, y, z
+  double fa[T::PMAX / 32], fcx[T::PMAX / 32], fcy[T::PMAX / 32], fcz[T::PMAX / 32];
+  unsigned ftouched = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) fa[k] = 0.0, fcx[k] = 0.0, fcy[k] = 0.0, fcz[k] = 0.0;
+  const int vl = lane / 6, tt = lane - 6 * (lane / 6);
+  for (int base = 0; base < nv; base += 5) {
+    const int v = base + vl;
+    const bool act = lane < 30 && v < nv;
+    D3 pr = {0.0, 0.0, 0.0};
+    bool ok = true;
+    int plane = 0;
+    D3 vloc = {0.0, 0.0, 0.0};
+    if (act) {
+      const int i = tt >> 1;
+      const int d0 = S.vd0[v], d1 = S.vd1[v], d2 = S.vd2[v];
+      const int cur = i == 0 ? d0 : (i == 1 ? d1 : d2);
+      const D3 cn = {S.pnx[cur], S.pny[cur], S.pnz[cur]};
+      if ((tt & 1) == 0) {
+        pr = plane_project(cn, {S.ppx[cur], S.ppy[cur], S.ppz[cur]}, x);
+      } else {
+        const int nx = i == 0 ? d1 : (i == 1 ? d2 : d0);
+        const D3 nn = {S.pnx[nx], S.pny[nx], S.pnz[nx]};
+        const D3 perp = cross(nn, cn);
+        ok = intersect3(nn, S.pd[nx], cn, S.pd[cur], perp, dot(x, perp), &pr);
+      }
+      plane = cur;
+      vloc = {S.vx[v], S.vy[v], S.vz[v]};
+    }
+    if (__any_sync(FULL, !ok)) {
+      *err_code = MV_ERR_DET;
+      return CELL_ERROR;
+    }
+    // proj[(t + 5) % 6] lives on lane 6 vl + (t + 5) % 6
+    const int src = 6 * vl + (tt + 5) % 6;
+    const int srcl = src < 32 ? src : lane;
+    D3 pq;
+    pq.x = __shfl_sync(FULL, pr.x, srcl);
+    pq.y = __shfl_sync(FULL, pr.y, srcl);
+    pq.z = __shfl_sync(FULL, pr.z, srcl);
+    if (act) {
+      const double vol = signed_volume_tet(pr, pq, vloc, x);
+      const D3 vc = scale(vol, add(add(add(pr, pq), vloc), x));
+      const double ar = signed_area_tri(pr, pq, vloc, x);
+      const D3 ac = scale(ar, add(add(pr, pq), vloc));
+      S.u.t.val[0][lane] = vol;
+      S.u.t.val[1][lane] = vc.x;
+      S.u.t.val[2][lane] = vc.y;
+      S.u.t.val[3][lane] = vc.z;
+      S.u.t.val[4][lane] = ar;
+      S.u.t.val[5][lane] = ac.x;
+      S.u.t.val[6][lane] = ac.y;
+      S.u.t.val[7][lane] = ac.z;
+      S.u.t.plane[lane] = plane;
+    }
+    __syncwarp();
+    const int ntet = 6 * min(5, nv - base);
+    if (lane < 4) {
+      for (int s = 0; s < ntet; s++) cacc = cacc + S.u.t.val[lane][s];
+    }
+#pragma unroll
+    for (int k = 0; k < T::PMAX / 32; k++) {
+      const int pl = lane + 32 * k;
+      if (pl < np) {
+        for (int s = 0; s < ntet; s++) {
+          if (S.u.t.plane[s] == pl) {
+            fa[k] = fa[k] + S.u.t.val[4][s];
+            fcx[k] = fcx[k] + S.u.t.val[5][s];
+            fcy[k] = fcy[k] + S.u.t.val[6][s];
+            fcz[k] = fcz[k] + S.u.t.val[7][s];
+            ftouched |= 1u << k;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // cell: VolumeCentroidIntegral::finalize (integrals.rs:97-105)
+  const double vol = __shfl_sync(FULL, cacc, 0);
+  const double nrm = vol > 0.0 ? 0.25 / vol : 0.0;
+  if (lane < 4 && lane > 0) J.centroid[3 * (int64_t)self + (lane - 1)] = cacc * nrm;
+  if (lane == 0) {
+    J.volume[self] = vol;
+    J.safety_radius[self] = sr;
+  }
+  // faces: ownership (voronoi_cell.rs:414-434) and emission in plane order
+  unsigned emit = 0;
+  int nf_mine = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) {
+    const int pl = lane + 32 * k;
+    bool e = false;
+    if (pl < np && ((ftouched >> k) & 1u)) {
+      const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
+      e = vector_is_valid(dim, nn);
+      const int r = S.pright[pl];
+      if (e && J.face_mode == MV_FACES_OWNED && r >= 0 && S.pcode[pl] == 13)
+        e = r > self || (J.mask != nullptr && J.mask[r] == 0);
+    }
+    emit |= (unsigned)e << k;
+    nf_mine += e;
+  }
+  int nf;
+  warp_excl_scan(nf_mine, lane, &nf);
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(J.face_counter, (unsigned long long)nf);
+  base = __shfl_sync(FULL, base, 0);
+  if ((long long)(base + nf) > J.face_cap) return CELL_FACE_OVERFLOW;  // host grows staging, reruns
+  if (lane == 0) {
+    J.face_count[self] = nf;
+    J.stage_off[self] = (int64_t)base;
+  }
+  int rank_base = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) {
+    const bool ek = (emit >> k) & 1u;
+    const unsigned bal = __ballot_sync(FULL, ek);
+    if (ek) {
+      const int pl = lane + 32 * k;
+      const int64_t f = (int64_t)base + rank_base + __popc(bal & lanemask_lt());
+      const double na = fa[k] > 0.0 ? 1.0 / (3.0 * fa[k]) : 0.0;
+      J.f_left[f] = self;
+      J.f_right[f] = S.pright[pl];
+      J.f_area[f] = fa[k];
+      J.f_centroid[3 * f] = fcx[k] * na;
+      J.f_centroid[3 * f + 1] = fcy[k] * na;
+      J.f_centroid[3 * f + 2] = fcz[k] * na;
+      J.f_normal[3 * f] = S.pnx[pl];
+      J.f_normal[3 * f + 1] = S.pny[pl];
+      J.f_normal[3 * f + 2] = S.pnz[pl];
+      J.f_code[f] = S.pcode[pl];
+    }
+    rank_base += __popc(bal);
+  }
+  WCNT(S, ST_CELLS, 1);
+  return CELL_DONE;
+}
+
+
 template <class T, int PREC>
 __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, const double* ext,
-                          WarpCounters& wc, int* err_code) {
+                          int* err_code) {
   using PIdx = typename T::PIdx;
   const int self = __ldg(J.sid + spos);
   const D3 x = load_gen(J, self);
@@ -533,10 +688,20 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   }
   __syncwarp();
   {
-    const int duals[8][3] = {{2, 5, 0}, {5, 3, 0}, {1, 5, 2}, {5, 1, 3},
-                             {4, 2, 0}, {4, 0, 3}, {2, 4, 1}, {4, 3, 1}};
+    // vertex duals of the cuboid (convex_cell.rs:298-307)
+    int i0 = 0, i1 = 0, i2 = 0;
+    switch (lane) {
+      case 0: i0 = 2, i1 = 5, i2 = 0; break;
+      case 1: i0 = 5, i1 = 3, i2 = 0; break;
+      case 2: i0 = 1, i1 = 5, i2 = 2; break;
+      case 3: i0 = 5, i1 = 1, i2 = 3; break;
+      case 4: i0 = 4, i1 = 2, i2 = 0; break;
+      case 5: i0 = 4, i1 = 0, i2 = 3; break;
+      case 6: i0 = 2, i1 = 4, i2 = 1; break;
+      default: i0 = 4, i1 = 3, i2 = 1; break;
+    }
     bool ok = true;
-    if (lane < 8) ok = make_vertex(S, lane, duals[lane][0], duals[lane][1], duals[lane][2], x, dim);
+    if (lane < 8) ok = make_vertex(S, lane, i0, i1, i2, x, dim);
     if (__any_sync(FULL, !ok)) {
       *err_code = MV_ERR_DET;
       return CELL_ERROR;
@@ -547,7 +712,6 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   double max_r2 = warp_max(lane < 8 ? S.vr2[lane] : -1.0);
   double sr = 2.0 * sqrt(max_r2);
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
-  const bool filt_ok = (PREC == MV_PRECISION_FILTERED) && x1 < 1e30;
 
   // ---- ConvexCell::build neighbour loop (convex_cell.rs:316-356) ----
   double R = J.R0;
@@ -555,7 +719,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   long long processed = 0;
   bool finished = false;
   for (int shell = 0; !finished; shell++) {
-    if (shell > 0) wc.c[ST_SHELLS]++;
+    if (shell > 0) WCNT(S, ST_SHELLS, 1);
     bool all;
     int cnt = gather_shell(J, S, lane, x, R, lo2, ext, &all);
     int shrink = 0;
@@ -591,63 +755,81 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         finished = true;
         break;
       }
-      wc.c[ST_NEIGHBOURS]++;
+      WCNT(S, ST_NEIGHBOURS, 1);
+
+      // Per-vertex decisions of clip_by_plane (convex_cell.rs:365-390).  rm: removed,
+      // und: not yet decided.  In filtered mode a division-free f32 test decides first:
+      //   sign(n.v - d) == sign((x - ngb).(v - x) + |x - ngb|^2 / 2)
+      // and |s32| > T certifies sign(clip64) with |clip64| >= errb, where T bounds the
+      // rounding of both the f32 evaluation and the reference's f64 plane.
+      unsigned rm[T::NW], und[T::NW];
+      bool need_plane = true;
+      const double A = amax_of(max_r2, dim);
+      const bool filt = (PREC == MV_PRECISION_FILTERED) && dist >= 1e-15 && dist <= 1e15 &&
+                        A <= 1e15 && x1 <= 1e15;
+      if (filt) {
+        const float ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y),
+                    ez = __double2float_rn(dx.z);
+        const float h32 = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        const double e1 = fabs(dx.x) + fabs(dx.y) + fabs(dx.z);
+        const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
+        const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
+        double Tb = dist * (errb_up + u64 * (11.0 * A + 11.0 * e1 + 14.0 * x1) +
+                            u32 * (5.02 * A + 4.03 * dist));
+        Tb = Tb * (1.0 + 1e-6) + 1e-40;
+        const float T32 = __double2float_ru(Tb);
+        unsigned any = 0;
+#pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int v = lane + 32 * w;
+          bool rem = false, un = false;
+          if (v < nv) {
+            const float s = fmaf(ez, S.fz[v], fmaf(ey, S.fy[v], fmaf(ex, S.fx[v], h32)));
+            const bool cert = fabsf(s) > T32;
+            rem = cert && s < 0.f;
+            un = !cert;
+          }
+          rm[w] = __ballot_sync(FULL, rem);
+          und[w] = __ballot_sync(FULL, un);
+          any |= rm[w] | und[w];
+        }
+        need_plane = any != 0;
+      } else {
+#pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int lim = nv - 32 * w;
+          rm[w] = 0u;
+          und[w] = lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
+        }
+      }
+      if (!need_plane) continue;  // certified: the half-space removes no vertex
+
       // HalfSpace::new (half_space.rs:24-34)
       const D3 n = divs(dx, dist);
       const D3 p = scale(0.5, add(x, ngb));
       const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
       const double d = dot(n, p);
-      // f32 filter constants (certifies sign(clip64) and |clip64| >= errb)
-      float n32x = 0.f, n32y = 0.f, n32z = 0.f, h32 = 0.f, thr32 = 0.f;
-      if (filt_ok) {
-        const double A = amax_of(max_r2, dim);
-        const double h = d - dot(n, x);
-        const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
-        double thr = errb + 6.0 * u32 * A + 5.0 * u32 * fabs(h) +
-                     9.0 * u64 * (fabs(d) + x1 + A) + 1e-40;
-        thr *= (1.0 + 1e-12);
-        n32x = __double2float_rn(n.x), n32y = __double2float_rn(n.y), n32z = __double2float_rn(n.z);
-        h32 = __double2float_rn(h);
-        thr32 = __double2float_ru(thr);
-        if (!(A < 1e30 && fabs(h) < 1e30)) thr32 = __int_as_float(0x7f800000);  // force f64
-      }
-      // clip test of every vertex (convex_cell.rs:365-390)
-      unsigned rm[T::NW];
       int n_und = 0, n_ex = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
+        n_und += __popc(und[w]);
         const int v = lane + 32 * w;
         bool removed = false;
-        if (v < nv) {
-          bool decided = false;
-          if (PREC == MV_PRECISION_FILTERED && filt_ok) {
-            const float c = fmaf(n32z, S.fz[v], fmaf(n32y, S.fy[v], fmaf(n32x, S.fx[v], -h32)));
-            if (fabsf(c) > thr32) {
-              removed = c < 0.f;
-              decided = true;
-            } else {
-              n_und++;
-            }
-          }
-          if (!decided) {
-            const double c = dot(n, D3{S.vx[v], S.vy[v], S.vz[v]}) - d;
-            if (fabs(c) < errb) {
-              removed = exact_clip(J, S, v, x, ngb) < 0;
-              n_ex++;
-            } else {
-              removed = c < 0.0;
-            }
+        if ((und[w] >> lane) & 1u) {
+          const double c = dot(n, D3{S.vx[v], S.vy[v], S.vz[v]}) - d;
+          if (fabs(c) < errb) {
+            removed = exact_clip(J, S, v, x, ngb) < 0;
+            n_ex++;
+          } else {
+            removed = c < 0.0;
           }
         }
-        rm[w] = __ballot_sync(FULL, removed);
+        rm[w] |= __ballot_sync(FULL, removed);
       }
+      if (PREC == MV_PRECISION_FILTERED) WCNT(S, ST_F32_UNDECIDED, filt ? n_und : 0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        n_und += __shfl_xor_sync(FULL, n_und, o);
-        n_ex += __shfl_xor_sync(FULL, n_ex, o);
-      }
-      wc.c[ST_F32_UNDECIDED] += n_und;
-      wc.c[ST_EXACT] += n_ex;
+      for (int o = 16; o > 0; o >>= 1) n_ex += __shfl_xor_sync(FULL, n_ex, o);
+      WCNT(S, ST_EXACT, n_ex);
       int nrem = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
@@ -664,7 +846,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         S.pcode[p_idx] = (uint8_t)code;
       }
       np++;
-      wc.c[ST_PLANES]++;
+      WCNT(S, ST_PLANES, 1);
 
       // swap-remove permutation as a closed form of the ballot
       unsigned km[T::NW];
@@ -677,56 +859,79 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         totK += __popc(km[w]);
       }
       const int nvf = totK;
-      // stage this lane's vertices in registers, then scatter
-      double svx[T::NW], svy[T::NW], svz[T::NW], sr2[T::NW];
-      float sfx[T::NW], sfy[T::NW], sfz[T::NW];
-      PIdx s0[T::NW], s1[T::NW], s2[T::NW];
       int dest[T::NW];
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
         const int v = lane + 32 * w;
-        dest[w] = -1;
+        int dd = -1;
         if (v < nv) {
-          svx[w] = S.vx[v], svy[w] = S.vy[v], svz[w] = S.vz[v], sr2[w] = S.vr2[v];
-          sfx[w] = S.fx[v], sfy[w] = S.fy[v], sfz[w] = S.fz[v];
-          s0[w] = S.vd0[v], s1[w] = S.vd1[v], s2[w] = S.vd2[v];
           const bool isrem = (rm[w] >> lane) & 1u;
           if (!isrem) {
-            if (v < nvf) {
-              dest[w] = v;
-            } else {
-              const int s = totK - rank_below<T::NW>(km, v);
-              dest[w] = select_bit<T::NW>(rm, s);
-            }
+            dd = v < nvf ? v : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, v));
+          } else if (v <= nvf) {
+            const int t = rank_below<T::NW>(rm, v) + 1;
+            dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
           } else {
-            if (v <= nvf) {
-              const int t = rank_below<T::NW>(rm, v) + 1;
-              const int kr = (t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2);
-              dest[w] = kr - 1;
-            } else {
-              dest[w] = v - 1;
-            }
+            dd = v - 1;
           }
         }
+        dest[w] = dd;
       }
-      __syncwarp();
+      // scatter field by field (few live registers); removed vertices keep only duals
+      auto scatter_d = [&](double* a, bool kept_only) {
+        double t[T::NW];
 #pragma unroll
-      for (int w = 0; w < T::NW; w++) {
-        const int dd = dest[w];
-        if (dd >= 0) {
-          if (dd < nvf) {
-            S.vx[dd] = svx[w], S.vy[dd] = svy[w], S.vz[dd] = svz[w], S.vr2[dd] = sr2[w];
-            S.fx[dd] = sfx[w], S.fy[dd] = sfy[w], S.fz[dd] = sfz[w];
-          }
-          S.vd0[dd] = s0[w], S.vd1[dd] = s1[w], S.vd2[dd] = s2[w];
+        for (int w = 0; w < T::NW; w++) {
+          const int v = lane + 32 * w;
+          t[w] = v < nv ? a[v] : 0.0;
         }
-      }
-      __syncwarp();
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < T::NW; w++)
+          if (dest[w] >= 0 && (!kept_only || dest[w] < nvf)) a[dest[w]] = t[w];
+        __syncwarp();
+      };
+      auto scatter_f = [&](float* a) {
+        float t[T::NW];
+#pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int v = lane + 32 * w;
+          t[w] = v < nv ? a[v] : 0.f;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < T::NW; w++)
+          if (dest[w] >= 0 && dest[w] < nvf) a[dest[w]] = t[w];
+        __syncwarp();
+      };
+      auto scatter_i = [&](PIdx* a) {
+        PIdx t[T::NW];
+#pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int v = lane + 32 * w;
+          t[w] = v < nv ? a[v] : (PIdx)0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < T::NW; w++)
+          if (dest[w] >= 0) a[dest[w]] = t[w];
+        __syncwarp();
+      };
+      scatter_d(S.vx, true);
+      scatter_d(S.vy, true);
+      scatter_d(S.vz, true);
+      scatter_d(S.vr2, true);
+      scatter_f(S.fx);
+      scatter_f(S.fy);
+      scatter_f(S.fz);
+      scatter_i(S.vd0);
+      scatter_i(S.vd1);
+      scatter_i(S.vd2);
 
       // ring of the removed region (compute_boundary + SimpleCycle iteration)
       int E = ring_parallel(S, lane, nvf, nv);
       if (E < 0) {
-        wc.c[ST_SERIAL_RING]++;
+        WCNT(S, ST_SERIAL_RING, 1);
         int e2 = 0;
         if (lane == 0) e2 = ring_serial(S, nvf, nv, np);
         E = __shfl_sync(FULL, e2, 0);
@@ -761,161 +966,18 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     R = fmax(R * 1.3, sr * 1.05);
   }
 
-  // ---- integrals (convex_cell.rs:131-187, voronoi_cell.rs:40-100) ----
-  // Tets go through 30-lane steps (5 vertices x 6 tets); lanes 0-3 sum the cell
-  // integrals and lane p owns face p (and p + 32k), all in the reference's tet order.
-  double cacc = 0.0;                  // lanes 0..3: volume, centroid x, y, z
-  double fa[T::PMAX / 32], fcx[T::PMAX / 32], fcy[T::PMAX / 32], fcz[T::PMAX / 32];
-  bool ftouched[T::PMAX / 32];
-#pragma unroll
-  for (int k = 0; k < T::PMAX / 32; k++) {
-    fa[k] = 0.0, fcx[k] = 0.0, fcy[k] = 0.0, fcz[k] = 0.0;
-    ftouched[k] = false;
-  }
-  const int vl = lane / 6, tt = lane - 6 * (lane / 6);
-  for (int base = 0; base < nv; base += 5) {
-    const int v = base + vl;
-    const bool act = lane < 30 && v < nv;
-    D3 pr = {0.0, 0.0, 0.0};
-    bool ok = true;
-    int plane = 0;
-    D3 vloc = {0.0, 0.0, 0.0};
-    if (act) {
-      const int dl[3] = {S.vd0[v], S.vd1[v], S.vd2[v]};
-      const int i = tt >> 1;
-      const int cur = dl[i];
-      const D3 cn = {S.pnx[cur], S.pny[cur], S.pnz[cur]};
-      const D3 cp = {S.ppx[cur], S.ppy[cur], S.ppz[cur]};
-      if ((tt & 1) == 0) {
-        pr = plane_project(cn, cp, x);
-      } else {
-        const int nx = dl[(i + 1) % 3];
-        const D3 nn = {S.pnx[nx], S.pny[nx], S.pnz[nx]};
-        const D3 perp = cross(nn, cn);
-        ok = intersect3(nn, S.pd[nx], cn, S.pd[cur], perp, dot(x, perp), &pr);
-      }
-      plane = cur;
-      vloc = {S.vx[v], S.vy[v], S.vz[v]};
-    }
-    if (__any_sync(FULL, !ok)) {
-      *err_code = MV_ERR_DET;
-      return CELL_ERROR;
-    }
-    // proj[(t + 5) % 6] lives on lane 6 vl + (t + 5) % 6
-    const int src = 6 * vl + (tt + 5) % 6;
-    D3 pq;
-    pq.x = __shfl_sync(FULL, pr.x, src < 32 ? src : lane);
-    pq.y = __shfl_sync(FULL, pr.y, src < 32 ? src : lane);
-    pq.z = __shfl_sync(FULL, pr.z, src < 32 ? src : lane);
-    if (act) {
-      const int slot = lane;
-      const double vol = signed_volume_tet(pr, pq, vloc, x);
-      const D3 vc = scale(vol, add(add(add(pr, pq), vloc), x));
-      const double ar = signed_area_tri(pr, pq, vloc, x);
-      const D3 ac = scale(ar, add(add(pr, pq), vloc));
-      S.u.t.val[0][slot] = vol;
-      S.u.t.val[1][slot] = vc.x;
-      S.u.t.val[2][slot] = vc.y;
-      S.u.t.val[3][slot] = vc.z;
-      S.u.t.val[4][slot] = ar;
-      S.u.t.val[5][slot] = ac.x;
-      S.u.t.val[6][slot] = ac.y;
-      S.u.t.val[7][slot] = ac.z;
-      S.u.t.plane[slot] = plane;
-    }
-    __syncwarp();
-    const int ntet = 6 * min(5, nv - base);
-    if (lane < 4) {
-      for (int s = 0; s < ntet; s++) cacc = cacc + S.u.t.val[lane][s];
-    }
-#pragma unroll
-    for (int k = 0; k < T::PMAX / 32; k++) {
-      const int pl = lane + 32 * k;
-      if (pl < np) {
-        for (int s = 0; s < ntet; s++) {
-          if (S.u.t.plane[s] == pl) {
-            fa[k] = fa[k] + S.u.t.val[4][s];
-            fcx[k] = fcx[k] + S.u.t.val[5][s];
-            fcy[k] = fcy[k] + S.u.t.val[6][s];
-            fcz[k] = fcz[k] + S.u.t.val[7][s];
-            ftouched[k] = true;
-          }
-        }
-      }
-    }
-    __syncwarp();
-  }
-  // cell: VolumeCentroidIntegral::finalize (integrals.rs:97-105)
-  const double vol = __shfl_sync(FULL, cacc, 0);
-  const double nrm = vol > 0.0 ? 0.25 / vol : 0.0;
-  if (lane < 4 && lane > 0) J.centroid[3 * (int64_t)self + (lane - 1)] = cacc * nrm;
-  if (lane == 0) {
-    J.volume[self] = vol;
-    J.safety_radius[self] = sr;
-  }
-  // faces: ownership (voronoi_cell.rs:414-434) and emission in plane order
-  bool emit[T::PMAX / 32];
-  int nf_mine = 0;
-#pragma unroll
-  for (int k = 0; k < T::PMAX / 32; k++) {
-    const int pl = lane + 32 * k;
-    bool e = false;
-    if (pl < np && ftouched[k]) {
-      const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
-      e = vector_is_valid(dim, nn);
-      const int r = S.pright[pl];
-      if (e && J.face_mode == MV_FACES_OWNED && r >= 0 && S.pcode[pl] == 13)
-        e = r > self || (J.mask != nullptr && J.mask[r] == 0);
-    }
-    emit[k] = e;
-    nf_mine += e;
-  }
-  int nf;
-  warp_excl_scan(nf_mine, lane, &nf);
-  unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(J.face_counter, (unsigned long long)nf);
-  base = __shfl_sync(FULL, base, 0);
-  if ((long long)(base + nf) > J.face_cap) return CELL_FACE_OVERFLOW;  // host grows staging, reruns
-  if (lane == 0) {
-    J.face_count[self] = nf;
-    J.stage_off[self] = (int64_t)base;
-  }
-  int rank_base = 0;
-#pragma unroll
-  for (int k = 0; k < T::PMAX / 32; k++) {
-    const unsigned bal = __ballot_sync(FULL, emit[k]);
-    if (emit[k]) {
-      const int pl = lane + 32 * k;
-      const int64_t f = (int64_t)base + rank_base + __popc(bal & lanemask_lt());
-      const double na = fa[k] > 0.0 ? 1.0 / (3.0 * fa[k]) : 0.0;
-      J.f_left[f] = self;
-      J.f_right[f] = S.pright[pl];
-      J.f_area[f] = fa[k];
-      J.f_centroid[3 * f] = fcx[k] * na;
-      J.f_centroid[3 * f + 1] = fcy[k] * na;
-      J.f_centroid[3 * f + 2] = fcz[k] * na;
-      J.f_normal[3 * f] = S.pnx[pl];
-      J.f_normal[3 * f + 1] = S.pny[pl];
-      J.f_normal[3 * f + 2] = S.pnz[pl];
-      J.f_code[f] = S.pcode[pl];
-    }
-    rank_base += __popc(bal);
-  }
-  wc.c[ST_CELLS]++;
-  return CELL_DONE;
+  return integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
 }
 
 template <class T, int PREC, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) cells_kernel(Job J) {
+__global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid_constant__ Job J) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   CellSmem<T>& S = reinterpret_cast<CellSmem<T>*>(smem_raw)[warp];
   __shared__ double ext_s[6];
   if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  if (lane < ST_COUNT) S.cnt[lane] = 0ull;
   __syncthreads();
-  WarpCounters wc;
-#pragma unroll
-  for (int i = 0; i < ST_COUNT; i++) wc.c[i] = 0;
   const int total = J.order ? J.n_order : J.n;
   for (;;) {
     int item = 0;
@@ -936,14 +998,14 @@ __global__ void __launch_bounds__(32 * WARPS) cells_kernel(Job J) {
       continue;
     }
     int err = 0;
-    const int res = build_cell<T, PREC>(J, S, lane, spos, ext_s, wc, &err);
+    const int res = build_cell<T, PREC>(J, S, lane, spos, ext_s, &err);
     __syncwarp();
     if (res == CELL_OVERFLOW) {
       if (lane == 0) {
         unsigned k = atomicAdd(J.ovf_count, 1u);
         J.ovf_list[k] = spos;
+        S.cnt[ST_OVERFLOW]++;
       }
-      wc.c[ST_OVERFLOW]++;
     } else if (res == CELL_FACE_OVERFLOW) {
       if (lane == 0) atomicExch(J.status + STATUS_FACE_OVERFLOW, 1);
     } else if (res == CELL_ERROR) {
@@ -952,15 +1014,13 @@ __global__ void __launch_bounds__(32 * WARPS) cells_kernel(Job J) {
         atomicMin(J.status + STATUS_CELL, self);
       }
     }
+    __syncwarp();
   }
-  if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < ST_COUNT; i++)
-      if (wc.c[i]) atomicAdd(J.stats + i, wc.c[i]);
-  }
+  __syncwarp();
+  if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J.stats + lane, S.cnt[lane]);
 }
 
-// ---------------------------------------------------------------- launchers --
+
 template <class T, int PREC, int WARPS>
 static cudaError_t launch_tier(const Job& J, int blocks, cudaStream_t st) {
   const size_t smem = sizeof(CellSmem<T>) * WARPS;
