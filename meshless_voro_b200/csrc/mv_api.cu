@@ -328,6 +328,14 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     J.ext = C->ext;
     J.R0 = s.R0;
+    for (int c = 0; c < 27; c++) {
+      const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
+      for (int i = 0; i < 3; i++) {
+        const double q = (double)(-m[i]) * s.width[i];
+        J.qshift[c][i] = q;
+        J.shift[c][i] = -q;
+      }
+    }
     for (int k = 0; k < 6; k++) {
       for (int i = 0; i < 3; i++) J.bn[k][i] = s.bn[k][i], J.bp[k][i] = s.bp[k][i];
       J.bd[k] = s.bd[k];

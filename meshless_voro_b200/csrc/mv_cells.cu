@@ -12,13 +12,20 @@
 // memory.  Every step keeps the reference's sequential semantics:
 //   * neighbours are consumed in ascending f64 squared distance (ties: original
 //     index, then shift code) from nested shells of a uniform grid;
-//   * the swap-remove loop of clip_by_plane is applied as a closed-form permutation
-//     derived from the ballot of removed vertices;
+//   * vertices sit in fixed slots; a byte array `ord` carries the reference's vertex
+//     order, and the swap-remove loop of clip_by_plane becomes a closed-form
+//     permutation of `ord` derived from the ballot of removed vertices;
 //   * the SimpleCycle ring is the boundary of the removed vertices' dual triangles,
 //     started where the reference starts it (serial replay when that node vanished);
 //   * cell and face integrals are summed in the reference's tet order.
 // Hence vertices, topology and integrals are the same binary64 values the
 // reference computes.
+//
+// Filtered precision tests a batch of upcoming neighbours at once with a
+// division-free f32 predicate whose error bound certifies the reference's f64
+// decision; neighbours certified to remove no vertex are consumed without building
+// their f64 bisector plane, and the first neighbour that needs attention gets the
+// reference's f64 (and, when undecided, exact integer) treatment.
 #include <cstdint>
 
 #include "../../include/mvgpu.h"
@@ -30,25 +37,30 @@ namespace mv {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-template <int VMAX_, int PMAX_, int CMAX_, typename PIdx_, int MINB_>
+template <int VMAX_, int PMAX_, int CMAX_, int KMAX_, typename PIdx_, int MINB_>
 struct Tier {
   static constexpr int MINB = MINB_;  // min resident blocks per SM (register budget)
-  static constexpr int VMAX = VMAX_;
-  static constexpr int PMAX = PMAX_;
-  static constexpr int CMAX = CMAX_;
-  static constexpr int NW = VMAX / 32;  // vertex mask words
+  static constexpr int VMAX = VMAX_;  // vertices
+  static constexpr int PMAX = PMAX_;  // clipping planes
+  static constexpr int CMAX = CMAX_;  // neighbour-shell entries
+  static constexpr int KMAX = KMAX_;  // neighbours set up per batch
+  static constexpr int NW = VMAX / 32;
   using PIdx = PIdx_;
   static constexpr unsigned NONE = (unsigned)(PIdx)(~0u);
   static_assert(VMAX % 32 == 0 && PMAX % 32 == 0 && CMAX % 32 == 0, "tier sizes");
-  static_assert(PMAX < (int)NONE, "plane index type too small");
+  static_assert(PMAX < (int)NONE && VMAX < (int)NONE, "index type too small");
+  static_assert(KMAX <= 32, "batch is set up by one lane per neighbour");
 };
 
 // Resident blocks per SM the fast tier is compiled for (sets its register budget).
 #ifndef MV_FAST_MINB
 #define MV_FAST_MINB 4
 #endif
-using TierFast = Tier<64, 64, 128, uint8_t, MV_FAST_MINB>;
-using TierLarge = Tier<512, 512, 512, uint16_t, 1>;
+#ifndef MV_FAST_KMAX
+#define MV_FAST_KMAX 16
+#endif
+using TierFast = Tier<64, 64, 128, MV_FAST_KMAX, uint8_t, MV_FAST_MINB>;
+using TierLarge = Tier<512, 512, 512, 32, uint16_t, 1>;
 
 template <class T>
 struct CellSmem {
@@ -60,23 +72,33 @@ struct CellSmem {
   int32_t pright[T::PMAX];  // original index of the right generator, -1: boundary
   uint8_t pcode[T::PMAX];   // periodic shift code, 13: none
   PIdx rptr[T::PMAX];       // ring successor (SimpleCycle::ptrs)
-  // vertices (convex_cell.rs:16-25), reference order
+  // vertices (convex_cell.rs:16-25) in fixed slots
   double vx[T::VMAX], vy[T::VMAX], vz[T::VMAX], vr2[T::VMAX];
   float fx[T::VMAX], fy[T::VMAX], fz[T::VMAX];  // f32 (v - x) for the filter
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
+  PIdx ord[T::VMAX];              // position -> slot; [0, nv) is the reference's order
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
   unsigned long long cnt[ST_COUNT];  // per-warp counters (flushed at exit)
   union {
-    struct {
-      unsigned long long key[T::CMAX];
-      uint32_t tie[T::CMAX];
+    struct {  // clipping phase
+      unsigned long long key[T::CMAX];  // f64 squared distance bits
+      uint32_t tie[T::CMAX];            // original index * 27 + shift code
+      int32_t cpos[T::CMAX];            // grid-sorted position of the generator
       int32_t sstart[96];
       int32_t spref[97];
       uint8_t scode[96];
+      // neighbours of the current batch
+      float bex[T::KMAX], bey[T::KMAX], bez[T::KMAX], bh[T::KMAX], bT[T::KMAX];
+      double bdx[T::KMAX], bdy[T::KMAX], bdz[T::KMAX], bdist[T::KMAX];
+      double bgx[T::KMAX], bgy[T::KMAX], bgz[T::KMAX];
+      int32_t borig[T::KMAX];
+      uint8_t bcode[T::KMAX];
+      uint8_t bfilt[T::KMAX];
     } g;
-    struct {
+    struct {  // integration phase
+      double px[T::PMAX], py[T::PMAX], pz[T::PMAX];  // generator projected on each plane
+      double ix[15], iy[15], iz[15];                 // on the plane-pair lines of 5 vertices
       double val[8][32];
-      int32_t plane[32];
     } t;
   } u;
 };
@@ -130,6 +152,11 @@ __device__ __forceinline__ int select_bit(const unsigned (&m)[NW], int s) {
   return -1;
 }
 
+__device__ __forceinline__ unsigned valid_bits(int nv, int w) {
+  const int lim = nv - 32 * w;
+  return lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
+}
+
 __device__ __forceinline__ void iloc(const Job& J, D3 l, int64_t out[3]) {
   const uint64_t mask = 0xFFFFFFFFFFFFFull;
   double c0 = 1.0 + (l.x - J.iloc_a[0]) * J.iloc_inv[0];
@@ -152,29 +179,30 @@ __device__ __forceinline__ D3 right_loc(const Job& J, const CellSmem<T>& S, int 
   if (r >= 0) {
     D3 l = load_gen(J, r);
     int code = S.pcode[k];
-    if (code != 13) l = add(l, shift_of_code(code, J.gw));
+    if (code != 13) l = add(l, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
     return l;
   }
   D3 pr = plane_project({S.pnx[k], S.pny[k], S.pnz[k]}, {S.ppx[k], S.ppy[k], S.ppz[k]}, x);
   return sub(scale(2.0, pr), x);
 }
 
-// Exact decision of clip_by_plane for an undecided vertex (convex_cell.rs:370-382).
+// Exact decision of clip_by_plane for an undecided vertex in slot `s`
+// (convex_cell.rs:370-382).
 template <class T>
-__device__ __noinline__ int exact_clip(const Job& J, const CellSmem<T>& S, int v, D3 x, D3 ngb) {
+__device__ __noinline__ int exact_clip(const Job& J, const CellSmem<T>& S, int s, D3 x, D3 ngb) {
   int64_t A[3], B[3], C[3], Dd[3], W[3];
   iloc(J, x, A);
-  iloc(J, right_loc(J, S, S.vd0[v], x), B);
-  iloc(J, right_loc(J, S, S.vd1[v], x), C);
-  iloc(J, right_loc(J, S, S.vd2[v], x), Dd);
+  iloc(J, right_loc(J, S, S.vd0[s], x), B);
+  iloc(J, right_loc(J, S, S.vd1[s], x), C);
+  iloc(J, right_loc(J, S, S.vd2[s], x), Dd);
   iloc(J, ngb, W);
   return in_sphere_exact_sign(A, B, C, Dd, W);
 }
 
-// Vertex::from_dual (convex_cell.rs:28-48); writes vertex slot `slot`.
+// Vertex::from_dual (convex_cell.rs:28-48) into slot `slot`.
 template <class T>
 __device__ __noinline__ bool make_vertex(CellSmem<T>& S, int slot, int i, int j, int k, D3 x,
-                                            int dim) {
+                                         int dim) {
   D3 loc;
   bool ok = intersect3({S.pnx[i], S.pny[i], S.pnz[i]}, S.pd[i], {S.pnx[j], S.pny[j], S.pnz[j]},
                        S.pd[j], {S.pnx[k], S.pny[k], S.pnz[k]}, S.pd[k], &loc);
@@ -212,8 +240,8 @@ enum CellResult { CELL_DONE = 0, CELL_OVERFLOW = 1, CELL_ERROR = 2, CELL_FACE_OV
 // (g - q).length_squared() for nn_iter (rstar) and |(q + s) - g|^2 for
 // wrapping_nn_iter (rtree_nn.rs:138-146).
 template <class T>
-__device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane, D3 x, double R, double lo2,
-                            const double* ext, bool* exhausted) {
+__device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane, D3 x, double R,
+                                         double lo2, const double* ext, bool* exhausted) {
   const double xa[3] = {x.x, x.y, x.z};
   int lo[3], hi[3];
   bool all = true;
@@ -252,8 +280,8 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
   for (int row0 = 0; row0 < nrows; row0 += 32) {
     const int row = row0 + lane;
     int nseg = 0;
-    int32_t s0[3] = {0, 0, 0}, sl[3] = {0, 0, 0};
-    int sc[3] = {0, 0, 0};
+    int32_t s0a = 0, s0b = 0, s0c = 0, sla = 0, slb = 0, slc = 0;
+    int sca = 0, scb = 0, scc = 0;
     if (row < nrows) {
       const int uy = lo[1] + row % ny, uz = lo[2] + row / ny;
       const double dy = box_d(1, uy), dz = box_d(2, uz);
@@ -279,9 +307,14 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
           int32_t ps = __ldg(J.cell_start + rowbase + c0);
           int32_t pe = __ldg(J.cell_start + rowbase + c1 + 1);
           if (pe > ps) {
-            s0[nseg] = ps;
-            sl[nseg] = pe - ps;
-            sc[nseg] = (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+            const int code = (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+            if (nseg == 0) {
+              s0a = ps, sla = pe - ps, sca = code;
+            } else if (nseg == 1) {
+              s0b = ps, slb = pe - ps, scb = code;
+            } else {
+              s0c = ps, slc = pe - ps, scc = code;
+            }
             nseg++;
           }
         }
@@ -289,17 +322,19 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
     }
     int nsegs_total;
     const int segoff = warp_excl_scan(nseg, lane, &nsegs_total);
-    const int mylen = sl[0] + sl[1] + sl[2];
+    const int mylen = sla + slb + slc;
     int total;
     const int lenoff = warp_excl_scan(mylen, lane, &total);
-    {
-      int run = lenoff;
-      for (int k = 0; k < nseg; k++) {
-        S.u.g.sstart[segoff + k] = s0[k];
-        S.u.g.spref[segoff + k] = run;
-        S.u.g.scode[segoff + k] = (uint8_t)sc[k];
-        run += sl[k];
-      }
+    if (nseg > 0) {
+      S.u.g.sstart[segoff] = s0a, S.u.g.spref[segoff] = lenoff, S.u.g.scode[segoff] = (uint8_t)sca;
+    }
+    if (nseg > 1) {
+      S.u.g.sstart[segoff + 1] = s0b, S.u.g.spref[segoff + 1] = lenoff + sla;
+      S.u.g.scode[segoff + 1] = (uint8_t)scb;
+    }
+    if (nseg > 2) {
+      S.u.g.sstart[segoff + 2] = s0c, S.u.g.spref[segoff + 2] = lenoff + sla + slb;
+      S.u.g.scode[segoff + 2] = (uint8_t)scc;
     }
     __syncwarp();
     for (int t0 = 0; t0 < total; t0 += 32) {
@@ -307,6 +342,7 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
       bool keep = false;
       double d2 = 0.0;
       uint32_t tie = 0;
+      int s = 0;
       if (t < total) {
         int a = 0, b = nsegs_total - 1;
         while (a < b) {
@@ -316,15 +352,14 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
           else
             b = mid - 1;
         }
-        const int s = S.u.g.sstart[a] + (t - S.u.g.spref[a]);
+        s = S.u.g.sstart[a] + (t - S.u.g.spref[a]);
         const int code = S.u.g.scode[a];
         const double px = __ldg(J.sx + s), py = __ldg(J.sy + s), pz = __ldg(J.sz + s);
         const int orig = __ldg(J.sid + s);
         if (J.periodic) {
-          const int mx = code % 3 - 1, my = (code / 3) % 3 - 1, mz = code / 9 - 1;
-          const double ddx = (x.x + (double)(-mx) * J.gw[0]) - px;
-          const double ddy = (x.y + (double)(-my) * J.gw[1]) - py;
-          const double ddz = (x.z + (double)(-mz) * J.gw[2]) - pz;
+          const double ddx = (x.x + J.qshift[code][0]) - px;
+          const double ddy = (x.y + J.qshift[code][1]) - py;
+          const double ddz = (x.z + J.qshift[code][2]) - pz;
           d2 = ddx * ddx + ddy * ddy + ddz * ddz;
         } else {
           D3 dd = sub(D3{px, py, pz}, x);
@@ -339,6 +374,7 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
       if (keep && pos < T::CMAX) {
         S.u.g.key[pos] = (unsigned long long)__double_as_longlong(d2);
         S.u.g.tie[pos] = tie;
+        S.u.g.cpos[pos] = s;
       }
       count += __popc(bal);
     }
@@ -348,7 +384,7 @@ __device__ __noinline__ int gather_shell(const Job& J, CellSmem<T>& S, int lane,
   return count;
 }
 
-// Bitonic sort of S.u.g.(key, tie)[0, n) ascending; n <= CMAX, padded to a power of 2.
+// Bitonic sort of the shell [0, n) by (key, tie) ascending, carrying cpos; n <= CMAX.
 template <class T>
 __device__ __noinline__ void sort_shell(CellSmem<T>& S, int lane, int n) {
   int np2 = 32;
@@ -356,6 +392,7 @@ __device__ __noinline__ void sort_shell(CellSmem<T>& S, int lane, int n) {
   for (int i = n + lane; i < np2; i += 32) {
     S.u.g.key[i] = ~0ull;
     S.u.g.tie[i] = ~0u;
+    S.u.g.cpos[i] = 0;
   }
   __syncwarp();
   for (int k = 2; k <= np2; k <<= 1) {
@@ -368,10 +405,13 @@ __device__ __noinline__ void sort_shell(CellSmem<T>& S, int lane, int n) {
         const uint32_t ta = S.u.g.tie[lo], tb = S.u.g.tie[hi];
         const bool gt = (ka > kb) || (ka == kb && ta > tb);
         if (gt == asc) {
+          const int32_t pa = S.u.g.cpos[lo], pb = S.u.g.cpos[hi];
           S.u.g.key[lo] = kb;
           S.u.g.key[hi] = ka;
           S.u.g.tie[lo] = tb;
           S.u.g.tie[hi] = ta;
+          S.u.g.cpos[lo] = pb;
+          S.u.g.cpos[hi] = pa;
         }
       }
       __syncwarp();
@@ -381,17 +421,19 @@ __device__ __noinline__ void sort_shell(CellSmem<T>& S, int lane, int n) {
 
 // -------------------------------------------------------------------- ring --
 // Serial replay of compute_boundary (convex_cell.rs:421-441) and SimpleCycle
-// (simple_cycle.rs:17-78) on lane 0 for the removed vertices at [nvf, nv).
-// Produces the edge list (S.ea, S.eb) and returns its length, or -1 on failure.
+// (simple_cycle.rs:17-78) on lane 0 for the removed vertices at positions [nvf, nv).
+// Produces the edge list (S.ea, S.eb) and returns its length, -1 on failure, -2 when
+// the ring exceeds the tier's vertex capacity.
 template <class T>
 __device__ __noinline__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np) {
   using PIdx = typename T::PIdx;
   for (int i = 0; i < np; i++) S.rptr[i] = (PIdx)i;
   auto contains = [&](int i) { return S.rptr[i] != (PIdx)i; };
-  int start = S.vd0[nvf];
+  const int s0 = S.ord[nvf];
+  int start = S.vd0[s0];
   int len = 3;
   {
-    int a = S.vd0[nvf], b = S.vd1[nvf], c = S.vd2[nvf];
+    int a = S.vd0[s0], b = S.vd1[s0], c = S.vd2[s0];
     S.rptr[a] = (PIdx)b;
     S.rptr[b] = (PIdx)c;
     S.rptr[c] = (PIdx)a;
@@ -401,32 +443,36 @@ __device__ __noinline__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np)
     int idx = i;
     for (;;) {
       if (idx >= n) return -1;
-      const int v = nvf + idx;
-      const int tri[3] = {S.vd0[v], S.vd1[v], S.vd2[v]};
-      const bool in[3] = {contains(tri[0]), contains(tri[1]), contains(tri[2])};
+      const int sl = S.ord[nvf + idx];
+      const int t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
+      const bool i0 = contains(t0), i1 = contains(t1), i2 = contains(t2);
       bool ok = false;
       for (int a = 0; a < 3 && !ok; a++) {
-        const int b = (a + 1) % 3, c = (a + 2) % 3;
-        if (!in[a] && in[b] && in[c] && S.rptr[tri[c]] == (PIdx)tri[b]) {
-          S.rptr[tri[c]] = (PIdx)tri[a];
-          S.rptr[tri[a]] = (PIdx)tri[b];
+        // rotation (ta, tb, tc) = (tri[a], tri[a+1], tri[a+2])
+        const int ta = a == 0 ? t0 : (a == 1 ? t1 : t2);
+        const int tb = a == 0 ? t1 : (a == 1 ? t2 : t0);
+        const int tc = a == 0 ? t2 : (a == 1 ? t0 : t1);
+        const bool ia = a == 0 ? i0 : (a == 1 ? i1 : i2);
+        const bool ib = a == 0 ? i1 : (a == 1 ? i2 : i0);
+        const bool ic = a == 0 ? i2 : (a == 1 ? i0 : i1);
+        if (!ia && ib && ic && S.rptr[tc] == (PIdx)tb) {
+          S.rptr[tc] = (PIdx)ta;
+          S.rptr[ta] = (PIdx)tb;
           len += 1;
           ok = true;
-        } else if (in[a] && in[b] && in[c] && S.rptr[tri[c]] == (PIdx)tri[b] &&
-                   S.rptr[tri[b]] == (PIdx)tri[a]) {
-          S.rptr[tri[c]] = (PIdx)tri[a];
-          S.rptr[tri[b]] = (PIdx)tri[b];
-          if (start == tri[b]) start = tri[a];
+        } else if (ia && ib && ic && S.rptr[tc] == (PIdx)tb && S.rptr[tb] == (PIdx)ta) {
+          S.rptr[tc] = (PIdx)ta;
+          S.rptr[tb] = (PIdx)tb;
+          if (start == tb) start = ta;
           len -= 1;
           ok = true;
         }
       }
       if (ok) {
         if (idx > i) {
-          const int w = nvf + i;
-          PIdx t0 = S.vd0[w], t1 = S.vd1[w], t2 = S.vd2[w];
-          S.vd0[w] = S.vd0[v], S.vd1[w] = S.vd1[v], S.vd2[w] = S.vd2[v];
-          S.vd0[v] = t0, S.vd1[v] = t1, S.vd2[v] = t2;
+          const PIdx tmp = S.ord[nvf + i];
+          S.ord[nvf + i] = S.ord[nvf + idx];
+          S.ord[nvf + idx] = tmp;
         }
         break;
       }
@@ -452,48 +498,37 @@ template <class T>
 __device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
   using PIdx = typename T::PIdx;
   const int r = nv - nvf;
-  for (int q = lane; q < r; q += 32) {
-    const int v = nvf + q;
-    S.rptr[S.vd0[v]] = (PIdx)T::NONE;
-    S.rptr[S.vd1[v]] = (PIdx)T::NONE;
-    S.rptr[S.vd2[v]] = (PIdx)T::NONE;
+  if (r > 32) return -1;  // large removal sets: the serial replay decides
+  int t0 = 0, t1 = 0, t2 = 0;
+  if (lane < r) {
+    const int sl = S.ord[nvf + lane];
+    t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
+    S.rptr[t0] = (PIdx)T::NONE;
+    S.rptr[t1] = (PIdx)T::NONE;
+    S.rptr[t2] = (PIdx)T::NONE;
   }
   __syncwarp();
-  int myedges = 0;
-  bool conflict = false;
-  int eu[3], ew[3];
-  for (int q = lane; q < r; q += 32) {
-    const int v = nvf + q;
-    const int t[3] = {S.vd0[v], S.vd1[v], S.vd2[v]};
-    for (int e = 0; e < 3; e++) {
-      const int u = t[e], w = t[(e + 1) % 3];
-      bool internal = false;
-      for (int k = 0; k < r && !internal; k++) {
-        if (k == q) continue;
-        const int o = nvf + k;
-        const int a = S.vd0[o], b = S.vd1[o], c = S.vd2[o];
-        internal = (a == w && b == u) || (b == w && c == u) || (c == w && a == u);
-      }
-      if (!internal) {
-        S.rptr[u] = (PIdx)w;
-        if (r <= 32) {
-          eu[myedges] = u;
-          ew[myedges] = w;
-        }
-        myedges++;
-      }
-    }
+  // an edge u->w of a removed triangle is on the boundary iff no other removed
+  // triangle holds w->u
+  bool b01 = lane < r, b12 = lane < r, b20 = lane < r;
+  for (int k = 0; k < r; k++) {
+    const int a = __shfl_sync(FULL, t0, k), b = __shfl_sync(FULL, t1, k),
+              c = __shfl_sync(FULL, t2, k);
+    if (k == lane) continue;
+    b01 = b01 && !((a == t1 && b == t0) || (b == t1 && c == t0) || (c == t1 && a == t0));
+    b12 = b12 && !((a == t2 && b == t1) || (b == t2 && c == t1) || (c == t2 && a == t1));
+    b20 = b20 && !((a == t0 && b == t2) || (b == t0 && c == t2) || (c == t0 && a == t2));
   }
+  if (b01) S.rptr[t0] = (PIdx)t1;
+  if (b12) S.rptr[t1] = (PIdx)t2;
+  if (b20) S.rptr[t2] = (PIdx)t0;
   __syncwarp();
-  if (r <= 32) {
-    for (int e = 0; e < myedges; e++) conflict |= (S.rptr[eu[e]] != (PIdx)ew[e]);
-  } else {
-    conflict = true;  // large removal sets: let the serial replay decide
-  }
+  bool conflict = (b01 && S.rptr[t0] != (PIdx)t1) || (b12 && S.rptr[t1] != (PIdx)t2) ||
+                  (b20 && S.rptr[t2] != (PIdx)t0);
   if (__any_sync(FULL, conflict)) return -1;
   int E;
-  warp_excl_scan(myedges, lane, &E);
-  const int start = S.vd0[nvf];
+  warp_excl_scan((int)b01 + (int)b12 + (int)b20, lane, &E);
+  const int start = S.vd0[S.ord[nvf]];
   if (S.rptr[start] == (PIdx)T::NONE) return -1;
   if (E > T::VMAX) return -1;
   int ok = 1;
@@ -518,64 +553,75 @@ __device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int
 
 // ------------------------------------------------------------------ the cell --
 // Per-warp counters live in shared memory (lane 0 updates them).
-#define WCNT(S, slot, v) \
-  do {                   \
+#define WCNT(S, slot, v)                                      \
+  do {                                                        \
     if (lane == 0) (S).cnt[slot] += (unsigned long long)(v); \
   } while (0)
 
 // Integrals and face emission of a finished cell (convex_cell.rs:131-187,
-// voronoi_cell.rs:40-100).  Tets go through 30-lane steps (5 vertices x 6 tets);
-// lanes 0-3 sum the cell integrals and lane p owns face p (and p + 32k), all in the
-// reference's tet order.
+// voronoi_cell.rs:40-100).  The generator's projection on each plane is computed
+// once per plane; each 5-vertex step projects on the 15 plane-pair lines, builds the
+// 30 tets (one per lane) and accumulates them in the reference's tet order: lanes
+// 0-3 the cell integrals, lane p (and p + 32k) the integrals of face p.
 template <class T>
 __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lane, int self, D3 x,
                                            int nv, int np, double sr, int* err_code) {
   const int dim = J.dim;
+  for (int pl = lane; pl < np; pl += 32) {
+    const D3 pr = plane_project({S.pnx[pl], S.pny[pl], S.pnz[pl]},
+                                {S.ppx[pl], S.ppy[pl], S.ppz[pl]}, x);
+    S.u.t.px[pl] = pr.x;
+    S.u.t.py[pl] = pr.y;
+    S.u.t.pz[pl] = pr.z;
+  }
   double cacc = 0.0;  // lanes 0..3: volume, centroid x, y, z
   double fa[T::PMAX / 32], fcx[T::PMAX / 32], fcy[T::PMAX / 32], fcz[T::PMAX / 32];
   unsigned ftouched = 0;
 #pragma unroll
   for (int k = 0; k < T::PMAX / 32; k++) fa[k] = 0.0, fcx[k] = 0.0, fcy[k] = 0.0, fcz[k] = 0.0;
-  const int vl = lane / 6, tt = lane - 6 * (lane / 6);
   for (int base = 0; base < nv; base += 5) {
-    const int v = base + vl;
-    const bool act = lane < 30 && v < nv;
-    D3 pr = {0.0, 0.0, 0.0};
+    const int nstep = min(5, nv - base);
+    // projections on the lines dual[i] & dual[i+1]: project_onto_intersection
+    // (geometry.rs:41-47) of plane dual[(i+1)%3] with dual[i]
     bool ok = true;
-    int plane = 0;
-    D3 vloc = {0.0, 0.0, 0.0};
-    if (act) {
-      const int i = tt >> 1;
-      const int d0 = S.vd0[v], d1 = S.vd1[v], d2 = S.vd2[v];
+    if (lane < 3 * nstep) {
+      const int vl = lane / 3, i = lane - 3 * vl;
+      const int sl = S.ord[base + vl];
+      const int d0 = S.vd0[sl], d1 = S.vd1[sl], d2 = S.vd2[sl];
       const int cur = i == 0 ? d0 : (i == 1 ? d1 : d2);
+      const int nx = i == 0 ? d1 : (i == 1 ? d2 : d0);
       const D3 cn = {S.pnx[cur], S.pny[cur], S.pnz[cur]};
-      if ((tt & 1) == 0) {
-        pr = plane_project(cn, {S.ppx[cur], S.ppy[cur], S.ppz[cur]}, x);
-      } else {
-        const int nx = i == 0 ? d1 : (i == 1 ? d2 : d0);
-        const D3 nn = {S.pnx[nx], S.pny[nx], S.pnz[nx]};
-        const D3 perp = cross(nn, cn);
-        ok = intersect3(nn, S.pd[nx], cn, S.pd[cur], perp, dot(x, perp), &pr);
-      }
-      plane = cur;
-      vloc = {S.vx[v], S.vy[v], S.vz[v]};
+      const D3 nn = {S.pnx[nx], S.pny[nx], S.pnz[nx]};
+      const D3 perp = cross(nn, cn);
+      D3 pr = {0.0, 0.0, 0.0};
+      ok = intersect3(nn, S.pd[nx], cn, S.pd[cur], perp, dot(x, perp), &pr);
+      S.u.t.ix[lane] = pr.x;
+      S.u.t.iy[lane] = pr.y;
+      S.u.t.iz[lane] = pr.z;
     }
     if (__any_sync(FULL, !ok)) {
       *err_code = MV_ERR_DET;
       return CELL_ERROR;
     }
-    // proj[(t + 5) % 6] lives on lane 6 vl + (t + 5) % 6
-    const int src = 6 * vl + (tt + 5) % 6;
-    const int srcl = src < 32 ? src : lane;
-    D3 pq;
-    pq.x = __shfl_sync(FULL, pr.x, srcl);
-    pq.y = __shfl_sync(FULL, pr.y, srcl);
-    pq.z = __shfl_sync(FULL, pr.z, srcl);
-    if (act) {
-      const double vol = signed_volume_tet(pr, pq, vloc, x);
-      const D3 vc = scale(vol, add(add(add(pr, pq), vloc), x));
-      const double ar = signed_area_tri(pr, pq, vloc, x);
-      const D3 ac = scale(ar, add(add(pr, pq), vloc));
+    __syncwarp();
+    // DecompositionWithoutFaces: tet t of a vertex = (proj[t], proj[(t+5)%6], vertex)
+    // with proj[2i] on plane dual[i] and proj[2i+1] on the line (dual[i+1], dual[i])
+    if (lane < 6 * nstep) {
+      const int vl = lane / 6, t = lane - 6 * vl;
+      const int sl = S.ord[base + vl];
+      const int d0 = S.vd0[sl], d1 = S.vd1[sl], d2 = S.vd2[sl];
+      auto proj = [&](int q) -> D3 {
+        const int i = q >> 1;
+        if (q & 1) return D3{S.u.t.ix[3 * vl + i], S.u.t.iy[3 * vl + i], S.u.t.iz[3 * vl + i]};
+        const int pl = i == 0 ? d0 : (i == 1 ? d1 : d2);
+        return D3{S.u.t.px[pl], S.u.t.py[pl], S.u.t.pz[pl]};
+      };
+      const D3 v0 = proj(t), v1 = proj(t == 0 ? 5 : t - 1);
+      const D3 vloc = {S.vx[sl], S.vy[sl], S.vz[sl]};
+      const double vol = signed_volume_tet(v0, v1, vloc, x);
+      const D3 vc = scale(vol, add(add(add(v0, v1), vloc), x));
+      const double ar = signed_area_tri(v0, v1, vloc, x);
+      const D3 ac = scale(ar, add(add(v0, v1), vloc));
       S.u.t.val[0][lane] = vol;
       S.u.t.val[1][lane] = vc.x;
       S.u.t.val[2][lane] = vc.y;
@@ -584,10 +630,9 @@ __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lan
       S.u.t.val[5][lane] = ac.x;
       S.u.t.val[6][lane] = ac.y;
       S.u.t.val[7][lane] = ac.z;
-      S.u.t.plane[lane] = plane;
     }
     __syncwarp();
-    const int ntet = 6 * min(5, nv - base);
+    const int ntet = 6 * nstep;
     if (lane < 4) {
       for (int s = 0; s < ntet; s++) cacc = cacc + S.u.t.val[lane][s];
     }
@@ -595,12 +640,19 @@ __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lan
     for (int k = 0; k < T::PMAX / 32; k++) {
       const int pl = lane + 32 * k;
       if (pl < np) {
-        for (int s = 0; s < ntet; s++) {
-          if (S.u.t.plane[s] == pl) {
+        for (int vl = 0; vl < nstep; vl++) {
+          const int sl = S.ord[base + vl];
+          const int kk = S.vd0[sl] == pl ? 0 : (S.vd1[sl] == pl ? 1 : (S.vd2[sl] == pl ? 2 : -1));
+          if (kk >= 0) {
+            const int s = 6 * vl + 2 * kk;
             fa[k] = fa[k] + S.u.t.val[4][s];
             fcx[k] = fcx[k] + S.u.t.val[5][s];
             fcy[k] = fcy[k] + S.u.t.val[6][s];
             fcz[k] = fcz[k] + S.u.t.val[7][s];
+            fa[k] = fa[k] + S.u.t.val[4][s + 1];
+            fcx[k] = fcx[k] + S.u.t.val[5][s + 1];
+            fcy[k] = fcy[k] + S.u.t.val[6][s + 1];
+            fcz[k] = fcz[k] + S.u.t.val[7][s + 1];
             ftouched |= 1u << k;
           }
         }
@@ -669,6 +721,61 @@ __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lan
   return CELL_DONE;
 }
 
+// Sets up neighbours [j, j + kb) of the sorted shell, one lane each: f64 location,
+// offset and distance as the reference computes them (convex_cell.rs:333-342), plus
+// the f32 quantities of the division-free filter.  Returns the ballots of neighbours
+// whose distance is degenerate (*bad) and of those beyond the safety radius (*stop).
+//
+// Filter: for a vertex v = x + a and e = x - ngb,
+//   s = e.a + |e|^2 / 2 = dist * M,   M = (n.v - d) up to the plane's rounding,
+// and |s32| > T certifies sign(clip64) with |clip64| >= errb, where
+//   T = dist * (errb_up + u64 (11 A + 11 |e|_1 + 14 |x|_1) + u32 (5.02 A + 4.03 dist))
+// bounds the f64 rounding of n = e / dist, p = (x + ngb) / 2, d = n.p and n.v - d
+// (u64 terms) and the f32 rounding of e, a and the three FMAs (u32 terms); A bounds
+// |a| over the cell's vertices.
+template <class T, int PREC>
+__device__ __forceinline__ void setup_batch(const Job& J, CellSmem<T>& S, int lane, int j, int kb,
+                                            D3 x, double x1, double sr, double A, unsigned* bad,
+                                            unsigned* stop) {
+  bool b = false, st = false;
+  if (lane < kb) {
+    const int c = j + lane;
+    const uint32_t tie = S.u.g.tie[c];
+    const int orig = (int)(tie / 27u);
+    const int code = (int)(tie - (uint32_t)orig * 27u);
+    const int sp = S.u.g.cpos[c];
+    D3 ngb = {__ldg(J.sx + sp), __ldg(J.sy + sp), __ldg(J.sz + sp)};
+    if (code != 13) ngb = add(ngb, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+    const D3 dx = sub(x, ngb);
+    const double dist = sqrt(dot(dx, dx));
+    b = !(dist > 0.0 && dist <= 1.7976931348623157e308);
+    st = !b && sr < dist;
+    S.u.g.bdx[lane] = dx.x, S.u.g.bdy[lane] = dx.y, S.u.g.bdz[lane] = dx.z;
+    S.u.g.bdist[lane] = dist;
+    S.u.g.bgx[lane] = ngb.x, S.u.g.bgy[lane] = ngb.y, S.u.g.bgz[lane] = ngb.z;
+    S.u.g.borig[lane] = orig;
+    S.u.g.bcode[lane] = (uint8_t)code;
+    bool filt = false;
+    if (PREC == MV_PRECISION_FILTERED) {
+      filt = dist >= 1e-15 && dist <= 1e15 && A <= 1e15 && x1 <= 1e15;
+      const float ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y),
+                  ez = __double2float_rn(dx.z);
+      const double e1 = fabs(dx.x) + fabs(dx.y) + fabs(dx.z);
+      const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
+      const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
+      double Tb = dist * (errb_up + u64 * (11.0 * A + 11.0 * e1 + 14.0 * x1) +
+                          u32 * (5.02 * A + 4.03 * dist));
+      Tb = Tb * (1.0 + 1e-6) + 1e-40;
+      S.u.g.bex[lane] = ex, S.u.g.bey[lane] = ey, S.u.g.bez[lane] = ez;
+      S.u.g.bh[lane] = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+      S.u.g.bT[lane] = __double2float_ru(Tb);
+    }
+    S.u.g.bfilt[lane] = filt;
+  }
+  *bad = __ballot_sync(FULL, b);
+  *stop = __ballot_sync(FULL, st);
+  __syncwarp();
+}
 
 template <class T, int PREC>
 __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, const double* ext,
@@ -686,6 +793,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     S.pright[lane] = -1;
     S.pcode[lane] = 13;
   }
+  for (int i = lane; i < T::VMAX; i += 32) S.ord[i] = (PIdx)i;
   __syncwarp();
   {
     // vertex duals of the cuboid (convex_cell.rs:298-307)
@@ -711,6 +819,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   int nv = 8, np = 6;
   double max_r2 = warp_max(lane < 8 ? S.vr2[lane] : -1.0);
   double sr = 2.0 * sqrt(max_r2);
+  double A = amax_of(max_r2, dim);
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
 
   // ---- ConvexCell::build neighbour loop (convex_cell.rs:316-356) ----
@@ -718,6 +827,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   double lo2 = 0.0;
   long long processed = 0;
   bool finished = false;
+  int K = 1;  // neighbours set up per batch (adapts to runs of non-clipping neighbours)
   for (int shell = 0; !finished; shell++) {
     if (shell > 0) WCNT(S, ST_SHELLS, 1);
     bool all;
@@ -732,103 +842,109 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     }
     if (cnt > T::CMAX) return CELL_OVERFLOW;
     sort_shell(S, lane, cnt);
-    for (int j = 0; j < cnt; j++) {
-      const uint32_t tie = S.u.g.tie[j];
-      const int orig = (int)(tie / 27u);
-      const int code = (int)(tie - (uint32_t)orig * 27u);
-      if (processed + j == 0) {
-        if (orig != self) {
-          *err_code = MV_ERR_DEGENERATE;
-          return CELL_ERROR;
-        }
-        continue;
-      }
-      D3 ngb = load_gen(J, orig);
-      if (code != 13) ngb = add(ngb, shift_of_code(code, J.gw));
-      const D3 dx = sub(x, ngb);
-      const double dist = sqrt(dot(dx, dx));
-      if (!(dist > 0.0 && dist <= 1.7976931348623157e308)) {
+    int j = 0;
+    if (processed == 0 && cnt > 0) {
+      // the first neighbour must be the generator itself (convex_cell.rs:325-329)
+      if ((int)(S.u.g.tie[0] / 27u) != self) {
         *err_code = MV_ERR_DEGENERATE;
         return CELL_ERROR;
       }
-      if (sr < dist) {
-        finished = true;
-        break;
+      j = 1;
+    }
+    while (j < cnt) {
+      const int kb = min(PREC == MV_PRECISION_FILTERED ? K : 1, cnt - j);
+      unsigned bad, stop;
+      setup_batch<T, PREC>(J, S, lane, j, kb, x, x1, sr, A, &bad, &stop);
+      const int fb = bad ? __ffs(bad) - 1 : kb, fs = stop ? __ffs(stop) - 1 : kb;
+      const int limit = min(fb, fs);
+      // first neighbour in [0, limit) that may remove a vertex
+      int kstar = limit;
+      for (int k = 0; k < limit; k++) {
+        bool need = !S.u.g.bfilt[k];
+        if (!need) {
+          const float ex = S.u.g.bex[k], ey = S.u.g.bey[k], ez = S.u.g.bez[k];
+          const float h = S.u.g.bh[k], Tk = S.u.g.bT[k];
+#pragma unroll
+          for (int w = 0; w < T::NW; w++) {
+            const int q = lane + 32 * w;
+            if (q < nv) {
+              const int sl = S.ord[q];
+              const float s = fmaf(ez, S.fz[sl], fmaf(ey, S.fy[sl], fmaf(ex, S.fx[sl], h)));
+              need = need || !(fabsf(s) > Tk) || s < 0.f;
+            }
+          }
+        }
+        if (__any_sync(FULL, need)) {
+          kstar = k;
+          break;
+        }
+      }
+      WCNT(S, ST_NEIGHBOURS, kstar);
+      if (kstar == limit) {
+        // neighbours [0, limit) remove nothing
+        j += limit;
+        if (limit < kb) {
+          if (fb <= fs) {
+            *err_code = MV_ERR_DEGENERATE;  // convex_cell.rs:342
+            return CELL_ERROR;
+          }
+          finished = true;  // safety radius reached (convex_cell.rs:343-345)
+          break;
+        }
+        K = min(2 * K, T::KMAX);
+        continue;
       }
       WCNT(S, ST_NEIGHBOURS, 1);
-
-      // Per-vertex decisions of clip_by_plane (convex_cell.rs:365-390).  rm: removed,
-      // und: not yet decided.  In filtered mode a division-free f32 test decides first:
-      //   sign(n.v - d) == sign((x - ngb).(v - x) + |x - ngb|^2 / 2)
-      // and |s32| > T certifies sign(clip64) with |clip64| >= errb, where T bounds the
-      // rounding of both the f32 evaluation and the reference's f64 plane.
-      unsigned rm[T::NW], und[T::NW];
-      bool need_plane = true;
-      const double A = amax_of(max_r2, dim);
-      const bool filt = (PREC == MV_PRECISION_FILTERED) && dist >= 1e-15 && dist <= 1e15 &&
-                        A <= 1e15 && x1 <= 1e15;
-      if (filt) {
-        const float ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y),
-                    ez = __double2float_rn(dx.z);
-        const float h32 = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-        const double e1 = fabs(dx.x) + fabs(dx.y) + fabs(dx.z);
-        const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
-        const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
-        double Tb = dist * (errb_up + u64 * (11.0 * A + 11.0 * e1 + 14.0 * x1) +
-                            u32 * (5.02 * A + 4.03 * dist));
-        Tb = Tb * (1.0 + 1e-6) + 1e-40;
-        const float T32 = __double2float_ru(Tb);
-        unsigned any = 0;
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int v = lane + 32 * w;
-          bool rem = false, un = false;
-          if (v < nv) {
-            const float s = fmaf(ez, S.fz[v], fmaf(ey, S.fy[v], fmaf(ex, S.fx[v], h32)));
-            const bool cert = fabsf(s) > T32;
-            rem = cert && s < 0.f;
-            un = !cert;
-          }
-          rm[w] = __ballot_sync(FULL, rem);
-          und[w] = __ballot_sync(FULL, un);
-          any |= rm[w] | und[w];
-        }
-        need_plane = any != 0;
-      } else {
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int lim = nv - 32 * w;
-          rm[w] = 0u;
-          und[w] = lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
-        }
-      }
-      if (!need_plane) continue;  // certified: the half-space removes no vertex
-
-      // HalfSpace::new (half_space.rs:24-34)
+      // ---- neighbour kstar: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
+      const D3 dx = {S.u.g.bdx[kstar], S.u.g.bdy[kstar], S.u.g.bdz[kstar]};
+      const double dist = S.u.g.bdist[kstar];
+      const D3 ngb = {S.u.g.bgx[kstar], S.u.g.bgy[kstar], S.u.g.bgz[kstar]};
+      const int orig = S.u.g.borig[kstar];
+      const int code = S.u.g.bcode[kstar];
+      const bool filt = S.u.g.bfilt[kstar];
+      const float ex = S.u.g.bex[kstar], ey = S.u.g.bey[kstar], ez = S.u.g.bez[kstar];
+      const float h = S.u.g.bh[kstar], Tk = S.u.g.bT[kstar];
+      j += kstar + 1;
+      K = 1;
       const D3 n = divs(dx, dist);
       const D3 p = scale(0.5, add(x, ngb));
       const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
       const double d = dot(n, p);
+      unsigned rm[T::NW];
       int n_und = 0, n_ex = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
-        n_und += __popc(und[w]);
-        const int v = lane + 32 * w;
+        const int q = lane + 32 * w;
         bool removed = false;
-        if ((und[w] >> lane) & 1u) {
-          const double c = dot(n, D3{S.vx[v], S.vy[v], S.vz[v]}) - d;
-          if (fabs(c) < errb) {
-            removed = exact_clip(J, S, v, x, ngb) < 0;
-            n_ex++;
-          } else {
-            removed = c < 0.0;
+        if (q < nv) {
+          const int sl = S.ord[q];
+          bool decided = false;
+          if (PREC == MV_PRECISION_FILTERED && filt) {
+            const float s = fmaf(ez, S.fz[sl], fmaf(ey, S.fy[sl], fmaf(ex, S.fx[sl], h)));
+            if (fabsf(s) > Tk) {
+              removed = s < 0.f;
+              decided = true;
+            }
+          }
+          if (!decided) {
+            n_und++;
+            const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
+            if (fabs(c) < errb) {
+              removed = exact_clip(J, S, sl, x, ngb) < 0;
+              n_ex++;
+            } else {
+              removed = c < 0.0;
+            }
           }
         }
-        rm[w] |= __ballot_sync(FULL, removed);
+        rm[w] = __ballot_sync(FULL, removed);
       }
-      if (PREC == MV_PRECISION_FILTERED) WCNT(S, ST_F32_UNDECIDED, filt ? n_und : 0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) n_ex += __shfl_xor_sync(FULL, n_ex, o);
+      for (int o = 16; o > 0; o >>= 1) {
+        n_und += __shfl_xor_sync(FULL, n_und, o);
+        n_ex += __shfl_xor_sync(FULL, n_ex, o);
+      }
+      if (PREC == MV_PRECISION_FILTERED) WCNT(S, ST_F32_UNDECIDED, n_und);
       WCNT(S, ST_EXACT, n_ex);
       int nrem = 0;
 #pragma unroll
@@ -848,85 +964,42 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
       np++;
       WCNT(S, ST_PLANES, 1);
 
-      // swap-remove permutation as a closed form of the ballot
+      // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
       unsigned km[T::NW];
       int totK = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
-        const int lim = nv - 32 * w;
-        const unsigned valid = lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
-        km[w] = ~rm[w] & valid;
+        km[w] = ~rm[w] & valid_bits(nv, w);
         totK += __popc(km[w]);
       }
       const int nvf = totK;
-      int dest[T::NW];
+      {
+        int dest[T::NW];
+        PIdx held[T::NW];
 #pragma unroll
-      for (int w = 0; w < T::NW; w++) {
-        const int v = lane + 32 * w;
-        int dd = -1;
-        if (v < nv) {
-          const bool isrem = (rm[w] >> lane) & 1u;
-          if (!isrem) {
-            dd = v < nvf ? v : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, v));
-          } else if (v <= nvf) {
-            const int t = rank_below<T::NW>(rm, v) + 1;
-            dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
-          } else {
-            dd = v - 1;
+        for (int w = 0; w < T::NW; w++) {
+          const int q = lane + 32 * w;
+          int dd = -1;
+          held[w] = 0;
+          if (q < nv) {
+            held[w] = S.ord[q];
+            if (!((rm[w] >> lane) & 1u)) {
+              dd = q < nvf ? q : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, q));
+            } else if (q <= nvf) {
+              const int t = rank_below<T::NW>(rm, q) + 1;
+              dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
+            } else {
+              dd = q - 1;
+            }
           }
+          dest[w] = dd;
         }
-        dest[w] = dd;
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < T::NW; w++)
+          if (dest[w] >= 0) S.ord[dest[w]] = held[w];
+        __syncwarp();
       }
-      // scatter field by field (few live registers); removed vertices keep only duals
-      auto scatter_d = [&](double* a, bool kept_only) {
-        double t[T::NW];
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int v = lane + 32 * w;
-          t[w] = v < nv ? a[v] : 0.0;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int w = 0; w < T::NW; w++)
-          if (dest[w] >= 0 && (!kept_only || dest[w] < nvf)) a[dest[w]] = t[w];
-        __syncwarp();
-      };
-      auto scatter_f = [&](float* a) {
-        float t[T::NW];
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int v = lane + 32 * w;
-          t[w] = v < nv ? a[v] : 0.f;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int w = 0; w < T::NW; w++)
-          if (dest[w] >= 0 && dest[w] < nvf) a[dest[w]] = t[w];
-        __syncwarp();
-      };
-      auto scatter_i = [&](PIdx* a) {
-        PIdx t[T::NW];
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int v = lane + 32 * w;
-          t[w] = v < nv ? a[v] : (PIdx)0;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int w = 0; w < T::NW; w++)
-          if (dest[w] >= 0) a[dest[w]] = t[w];
-        __syncwarp();
-      };
-      scatter_d(S.vx, true);
-      scatter_d(S.vy, true);
-      scatter_d(S.vz, true);
-      scatter_d(S.vr2, true);
-      scatter_f(S.fx);
-      scatter_f(S.fy);
-      scatter_f(S.fz);
-      scatter_i(S.vd0);
-      scatter_i(S.vd1);
-      scatter_i(S.vd2);
 
       // ring of the removed region (compute_boundary + SimpleCycle iteration)
       int E = ring_parallel(S, lane, nvf, nv);
@@ -945,7 +1018,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
       if (nvf + E > T::VMAX) return CELL_OVERFLOW;
       bool ok = true;
       for (int e = lane; e < E; e += 32)
-        ok &= make_vertex(S, nvf + e, S.ea[e], S.eb[e], p_idx, x, dim);
+        ok &= make_vertex(S, S.ord[nvf + e], S.ea[e], S.eb[e], p_idx, x, dim);
       if (__any_sync(FULL, !ok)) {
         *err_code = MV_ERR_DET;
         return CELL_ERROR;
@@ -954,9 +1027,10 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
       nv = nvf + E;
       // update_safety_radius (convex_cell.rs:443-453)
       double m = -1.0;
-      for (int v = lane; v < nv; v += 32) m = fmax(m, S.vr2[v]);
+      for (int q = lane; q < nv; q += 32) m = fmax(m, S.vr2[S.ord[q]]);
       max_r2 = warp_max(m);
       sr = 2.0 * sqrt(max_r2);
+      A = amax_of(max_r2, dim);
     }
     if (finished) break;
     processed += cnt;
@@ -965,7 +1039,6 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     lo2 = R * R;
     R = fmax(R * 1.3, sr * 1.05);
   }
-
   return integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
 }
 
@@ -1020,6 +1093,20 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
   if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J.stats + lane, S.cnt[lane]);
 }
 
+// ---------------------------------------------------------------- launchers --
+constexpr int FAST_WARPS = 4;
+constexpr int LARGE_WARPS = 1;
+
+template <class T, int PREC, int WARPS>
+static int blocks_per_sm() {
+  int nb = 0;
+  const size_t smem = sizeof(CellSmem<T>) * WARPS;
+  auto k = cells_kernel<T, PREC, WARPS>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * WARPS, smem) != cudaSuccess) return 0;
+  return nb;
+}
 
 template <class T, int PREC, int WARPS>
 static cudaError_t launch_tier(const Job& J, int blocks, cudaStream_t st) {
@@ -1031,44 +1118,16 @@ static cudaError_t launch_tier(const Job& J, int blocks, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-constexpr int FAST_WARPS = 4;
-constexpr int LARGE_WARPS = 1;
-
-size_t cells_smem_fast() { return sizeof(CellSmem<TierFast>) * FAST_WARPS; }
-size_t cells_smem_large() { return sizeof(CellSmem<TierLarge>) * LARGE_WARPS; }
-
 int cells_blocks_per_sm_fast(int precision) {
-  int nb = 0;
-  const size_t smem = cells_smem_fast();
-  if (precision == MV_PRECISION_FILTERED) {
-    cudaFuncSetAttribute(cells_kernel<TierFast, MV_PRECISION_FILTERED, FAST_WARPS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &nb, cells_kernel<TierFast, MV_PRECISION_FILTERED, FAST_WARPS>, 32 * FAST_WARPS, smem);
-  } else {
-    cudaFuncSetAttribute(cells_kernel<TierFast, MV_PRECISION_FP64, FAST_WARPS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &nb, cells_kernel<TierFast, MV_PRECISION_FP64, FAST_WARPS>, 32 * FAST_WARPS, smem);
-  }
-  return nb;
+  return precision == MV_PRECISION_FILTERED
+             ? blocks_per_sm<TierFast, MV_PRECISION_FILTERED, FAST_WARPS>()
+             : blocks_per_sm<TierFast, MV_PRECISION_FP64, FAST_WARPS>();
 }
 
 int cells_blocks_per_sm_large(int precision) {
-  int nb = 0;
-  const size_t smem = cells_smem_large();
-  if (precision == MV_PRECISION_FILTERED) {
-    cudaFuncSetAttribute(cells_kernel<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &nb, cells_kernel<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>, 32 * LARGE_WARPS, smem);
-  } else {
-    cudaFuncSetAttribute(cells_kernel<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &nb, cells_kernel<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>, 32 * LARGE_WARPS, smem);
-  }
-  return nb;
+  return precision == MV_PRECISION_FILTERED
+             ? blocks_per_sm<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>()
+             : blocks_per_sm<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>();
 }
 
 cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st) {

@@ -68,6 +68,10 @@ struct Job {
   const double* ext;        // device [6]: min x,y,z, max x,y,z of the generators
   double geps[3];           // cell-box inflation against rounding of the cell index
   double R0;                // first neighbour-shell radius
+  // periodic image of shift code c = (mx+1) + 3(my+1) + 9(mz+1): the reference's query
+  // offset s = (-m) w (rtree_nn.rs:86) and emitted shift -s (rtree_nn.rs:27-33)
+  double qshift[27][3];
+  double shift[27][3];
   // ---- simulation boundary (boundary.rs:14-47) ----
   double bn[6][3];
   double bp[6][3];
