@@ -78,7 +78,7 @@ struct CellSmem {
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ord[T::VMAX];              // position -> slot; [0, nv) is the reference's order
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
-  unsigned long long cnt[ST_COUNT];  // per-warp counters (flushed at exit)
+  unsigned long long cnt[ST_COUNT];  // per-warp event counts (flushed to global at exit)
   union {
     struct {  // clipping phase
       unsigned long long key[T::CMAX];  // f64 squared distance bits
@@ -201,7 +201,7 @@ __device__ __noinline__ int exact_clip(const Job& J, const CellSmem<T>& S, int s
 
 // Vertex::from_dual (convex_cell.rs:28-48) into slot `slot`.
 template <class T>
-__device__ __noinline__ bool make_vertex(CellSmem<T>& S, int slot, int i, int j, int k, D3 x,
+__device__ __forceinline__ bool make_vertex(CellSmem<T>& S, int slot, int i, int j, int k, D3 x,
                                          int dim) {
   D3 loc;
   bool ok = intersect3({S.pnx[i], S.pny[i], S.pnz[i]}, S.pd[i], {S.pnx[j], S.pny[j], S.pnz[j]},
@@ -495,7 +495,7 @@ __device__ __noinline__ int ring_serial(CellSmem<T>& S, int nvf, int nv, int np)
 // vertex's dual[0] whenever that node is still on the boundary.  Returns the edge
 // count, or -1 when the serial replay must decide.
 template <class T>
-__device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
+__device__ __forceinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int nv) {
   using PIdx = typename T::PIdx;
   const int r = nv - nvf;
   if (r > 32) return -1;  // large removal sets: the serial replay decides
@@ -552,11 +552,12 @@ __device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int
 }
 
 // ------------------------------------------------------------------ the cell --
-// Per-warp counters live in shared memory (lane 0 updates them).
-#define WCNT(S, slot, v)                                      \
-  do {                                                        \
-    if (lane == 0) (S).cnt[slot] += (unsigned long long)(v); \
-  } while (0)
+// Event counts of one cell, kept in warp-uniform registers (a lane-0 branch inside
+// the clip loop would split the warp) and flushed once per cell.
+struct CellCount {
+  unsigned c[ST_COUNT];
+};
+#define WCNT(CC, slot, v) ((CC).c[slot] += (unsigned)(v))
 
 // Integrals and face emission of a finished cell (convex_cell.rs:131-187,
 // voronoi_cell.rs:40-100).  The generator's projection on each plane is computed
@@ -566,6 +567,7 @@ __device__ __noinline__ int ring_parallel(CellSmem<T>& S, int lane, int nvf, int
 template <class T>
 __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lane, int self, D3 x,
                                            int nv, int np, double sr, int* err_code) {
+  // (the cell count is taken by the caller)
   const int dim = J.dim;
   for (int pl = lane; pl < np; pl += 32) {
     const D3 pr = plane_project({S.pnx[pl], S.pny[pl], S.pnz[pl]},
@@ -717,7 +719,6 @@ __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lan
     }
     rank_base += __popc(bal);
   }
-  WCNT(S, ST_CELLS, 1);
   return CELL_DONE;
 }
 
@@ -779,7 +780,7 @@ __device__ __forceinline__ void setup_batch(const Job& J, CellSmem<T>& S, int la
 
 template <class T, int PREC>
 __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, const double* ext,
-                          int* err_code) {
+                          int* err_code, CellCount& cc) {
   using PIdx = typename T::PIdx;
   const int self = __ldg(J.sid + spos);
   const D3 x = load_gen(J, self);
@@ -829,7 +830,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   bool finished = false;
   int K = 1;  // neighbours set up per batch (adapts to runs of non-clipping neighbours)
   for (int shell = 0; !finished; shell++) {
-    if (shell > 0) WCNT(S, ST_SHELLS, 1);
+    if (shell > 0) WCNT(cc, ST_SHELLS, 1);
     bool all;
     int cnt = gather_shell(J, S, lane, x, R, lo2, ext, &all);
     int shrink = 0;
@@ -879,7 +880,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
           break;
         }
       }
-      WCNT(S, ST_NEIGHBOURS, kstar);
+      WCNT(cc, ST_NEIGHBOURS, kstar);
       if (kstar == limit) {
         // neighbours [0, limit) remove nothing
         j += limit;
@@ -894,7 +895,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         K = min(2 * K, T::KMAX);
         continue;
       }
-      WCNT(S, ST_NEIGHBOURS, 1);
+      WCNT(cc, ST_NEIGHBOURS, 1);
       // ---- neighbour kstar: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
       const D3 dx = {S.u.g.bdx[kstar], S.u.g.bdy[kstar], S.u.g.bdz[kstar]};
       const double dist = S.u.g.bdist[kstar];
@@ -944,8 +945,8 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         n_und += __shfl_xor_sync(FULL, n_und, o);
         n_ex += __shfl_xor_sync(FULL, n_ex, o);
       }
-      if (PREC == MV_PRECISION_FILTERED) WCNT(S, ST_F32_UNDECIDED, n_und);
-      WCNT(S, ST_EXACT, n_ex);
+      if (PREC == MV_PRECISION_FILTERED) WCNT(cc, ST_F32_UNDECIDED, n_und);
+      WCNT(cc, ST_EXACT, n_ex);
       int nrem = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
@@ -962,7 +963,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         S.pcode[p_idx] = (uint8_t)code;
       }
       np++;
-      WCNT(S, ST_PLANES, 1);
+      WCNT(cc, ST_PLANES, 1);
 
       // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
       unsigned km[T::NW];
@@ -1004,7 +1005,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
       // ring of the removed region (compute_boundary + SimpleCycle iteration)
       int E = ring_parallel(S, lane, nvf, nv);
       if (E < 0) {
-        WCNT(S, ST_SERIAL_RING, 1);
+        WCNT(cc, ST_SERIAL_RING, 1);
         int e2 = 0;
         if (lane == 0) e2 = ring_serial(S, nvf, nv, np);
         E = __shfl_sync(FULL, e2, 0);
@@ -1071,7 +1072,16 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
       continue;
     }
     int err = 0;
-    const int res = build_cell<T, PREC>(J, S, lane, spos, ext_s, &err);
+    CellCount cc;
+#pragma unroll
+    for (int i = 0; i < ST_COUNT; i++) cc.c[i] = 0u;
+    const int res = build_cell<T, PREC>(J, S, lane, spos, ext_s, &err, cc);
+    __syncwarp();
+    if (res == CELL_DONE) cc.c[ST_CELLS]++;
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < ST_COUNT; i++) S.cnt[i] += cc.c[i];
+    }
     __syncwarp();
     if (res == CELL_OVERFLOW) {
       if (lane == 0) {
