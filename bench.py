@@ -34,6 +34,26 @@ HBM_PEAK_FALLBACK = 6650.0
 BYTES_GEN, BYTES_CELL, BYTES_FACE, BYTES_CONN = 24, 40, 68, 4
 
 
+def rank_seed(rank: int, base: int = 3) -> int:
+    """Weak scaling: every rank tessellates its own independently seeded generator set."""
+    return base + rank
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """Slowest rank's time (the job's time); identity without a process group."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_cells_per_s(world: int, n_per_rank: int, ms_max: float) -> float:
+    """Whole-job throughput: all ranks' cells over the slowest rank's time."""
+    return world * n_per_rank / (ms_max * 1e-3)
+
+
 def workload(name: str, seed: int):
     from meshless_voro_b200 import workloads as W
     if name == "poisson_256":
@@ -157,9 +177,10 @@ def run_reference(args, rank, world):
     vals = []
     for _ in range(args.warmup):
         cpu_baseline(w, budget_s=2.0)
+    cb = None
     for _ in range(args.steps):
-        vals.append(cpu_baseline(w, budget_s=args.cpu_budget)["value"])
-    cb = cpu_baseline(w, budget_s=args.cpu_budget)
+        cb = cpu_baseline(w, budget_s=args.cpu_budget)
+        vals.append(cb["value"])
     v = float(np.median(vals))
     line = {"metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v,
@@ -207,7 +228,7 @@ def main():
         dist.init_process_group("nccl", device_id=dev,
                                 timeout=__import__("datetime").timedelta(seconds=120))
 
-    w = workload(args.workload, seed=3 + rank)
+    w = workload(args.workload, seed=rank_seed(rank))
     n = len(w["generators"])
     g_host = torch.from_numpy(np.ascontiguousarray(w["generators"])).pin_memory()
     g_dev = g_host.to(dev)
@@ -235,11 +256,7 @@ def main():
             cells_ms.append(stats["ms_cells"])
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, dev)
         if world > 1:
             dist.barrier()
         return ms, float(np.mean(cells_ms)), stats, out
@@ -248,14 +265,14 @@ def main():
         ms, cells_ms, stats, out = timed(args.precision, args.steps)
     clocks = clk.summary()
     F, Cn = int(out.n_faces), int(out.n_connections)
-    value = world * n / (ms * 1e-3)
+    value = aggregate_cells_per_s(world, n, ms)
 
     # plain FP64 kernel side by side (same workload, same step)
     other = None
     if not args.no_compare:
         o_prec = "fp64" if args.precision == "filtered" else "filtered"
         o_ms, o_cells_ms, o_stats, _ = timed(o_prec, max(2, args.steps // 2))
-        other = {"precision": o_prec, "value": world * n / (o_ms * 1e-3),
+        other = {"precision": o_prec, "value": aggregate_cells_per_s(world, n, o_ms),
                  "ms_per_step": o_ms, "cells_kernel_ms": o_cells_ms,
                  "f32_undecided": o_stats["f32_undecided"], "exact_tests": o_stats["exact_tests"]}
 
@@ -287,13 +304,9 @@ def main():
             h = e2e_step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        e_ms = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            t = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
         d2h = (8 + 24 + 8 + 8 + 4) * n + (4 + 4 + 8 + 24 + 24 + 1) * int(h.n_faces) + 4 * int(h.n_connections)
-        e2e = {"value": world * n / (e_ms * 1e-3), "unit": "cells/s",
+        e2e = {"value": aggregate_cells_per_s(world, n, e_ms), "unit": "cells/s",
                "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
 
     peak, peak_kind = measured_peaks()
