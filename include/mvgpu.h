@@ -166,6 +166,40 @@ int mv_voronoi_build_partial(const double* generators, const uint8_t* mask, int6
 
 void mv_voronoi_free(mv_voronoi* v);
 
+/* ---- build without allocating (no counterpart in the reference crate) ----
+ *
+ * For callers that cannot call cudaMalloc -- a host framework that has handed all
+ * device memory to its own pool allocator, code that must not trigger the implicit
+ * device synchronisation of cudaMalloc/cudaFree, or an embedding with a fixed memory
+ * plan.  Same result as mv_context_build_device, on the current device, but every
+ * scratch buffer lives in one fixed static device array inside the library, so the
+ * call allocates nothing.  That array (about 30 MB) is held by every GPU that loads
+ * the library until the process exits.
+ *
+ * Limits: at most MV_NOALLOC_MAX_GENERATORS generators (larger n returns
+ * MV_ERR_CAPACITY without touching the GPU) and at most
+ * MV_NOALLOC_FACES_PER_GENERATOR * MV_NOALLOC_MAX_GENERATORS staged faces.
+ *
+ * The caller passes device inputs and fills `out` with device pointers sized for n
+ * cells (cell_volume, cell_centroid, cell_safety_radius, and for MV_FACES_OWNED
+ * cell_face_offset, cell_face_count), face_capacity faces (face_left ... face_shift_code)
+ * and connection_capacity connections (cell_face_connections, MV_FACES_OWNED only).
+ * On return out->n_faces / out->n_connections hold the sizes the build needed; when
+ * they exceed the capacities the call returns MV_ERR_CAPACITY.  Runs on opts->stream
+ * (NULL: the legacy default stream) and returns when the result is complete.
+ *
+ * The first call on a device looks up the array's device address (once per device);
+ * make that first call before any stream capture.  All calls share the array and it
+ * keeps the previous call's contents (each call clears what must start at zero):
+ * calls that overlap on the GPU -- from several host threads or streams -- race on it
+ * and must be serialised by the caller. */
+#define MV_NOALLOC_MAX_GENERATORS 32768
+#define MV_NOALLOC_FACES_PER_GENERATOR 12
+int mv_voronoi_build_noalloc(const double* d_generators, const uint8_t* d_mask, int64_t n,
+                             const double anchor[3], const double width[3], int dimensionality,
+                             int periodic, const mv_options* opts, mv_device_voronoi* out,
+                             int64_t face_capacity, int64_t connection_capacity);
+
 /* The reference's shift vector for a face shift code (rtree_nn.rs:27-33): component i
  * is m_i * width_i for m_i != 0 and -0.0 for m_i == 0, with (m_x, m_y, m_z) decoded
  * from code = (m_x+1) + 3(m_y+1) + 9(m_z+1).  Code 13 (no shift) gives all -0.0. */

@@ -34,7 +34,7 @@ EXPORTED = (
     "mv_options_default", "mv_strerror", "mv_version", "mv_context_create",
     "mv_context_destroy", "mv_context_last_stats", "mv_context_build_device",
     "mv_context_build", "mv_voronoi_build", "mv_voronoi_build_partial", "mv_voronoi_free",
-    "mv_shift_from_code",
+    "mv_shift_from_code", "mv_voronoi_build_noalloc",
 )
 
 
@@ -127,6 +127,10 @@ def lib():
         L.mv_voronoi_free.restype = None
         L.mv_shift_from_code.argtypes = [C.c_int, dp, dp]
         L.mv_shift_from_code.restype = None
+        L.mv_voronoi_build_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, dp, dp, C.c_int,
+                                               C.c_int, C.POINTER(Options),
+                                               C.POINTER(DeviceVoronoi), C.c_int64, C.c_int64]
+        L.mv_voronoi_build_noalloc.restype = C.c_int
         _lib = L
     return _lib
 

@@ -38,6 +38,89 @@ void launch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, co
                      const int32_t* in_count, int32_t* cursor, int n, int32_t* conn, cudaStream_t st);
 }  // namespace mv
 
+namespace mv {
+
+
+// voronoi.rs:200-210 + boundary.rs:14-47 + the grid resolution.
+int make_setup(int64_t n, const double* anchor, const double* width, int dim, int periodic,
+               const mv_options& o, Setup* s) {
+  if (dim < 1 || dim > 3) return MV_ERR_ARG;
+  D3 a = {anchor[0], anchor[1], anchor[2]};
+  D3 w = {width[0], width[1], width[2]};
+  if (dim == 1) {
+    a.y = -0.5;
+    w.y = 1.0;
+  }
+  if (dim == 1 || dim == 2) {
+    a.z = -0.5;
+    w.z = 1.0;
+  }
+  const double aa[3] = {a.x, a.y, a.z}, ww[3] = {w.x, w.y, w.z};
+  for (int i = 0; i < 3; i++) {
+    if (!std::isfinite(aa[i]) || !std::isfinite(ww[i]) || !(ww[i] > 0.0)) return MV_ERR_ARG;
+    s->anchor[i] = aa[i];
+    s->width[i] = ww[i];
+  }
+  s->dim = dim;
+  s->periodic = periodic ? 1 : 0;
+  // SimulationBoundary::cuboid
+  D3 ba = a, bw = w;
+  if (periodic) {
+    ba.x -= bw.x;
+    bw.x *= 3.0;
+    if (dim >= 2) {
+      ba.y -= bw.y;
+      bw.y *= 3.0;
+    }
+    if (dim == 3) {
+      ba.z -= bw.z;
+      bw.z *= 3.0;
+    }
+  }
+  const D3 hi = add(ba, bw);
+  const D3 ns[6] = {{1.0, 0.0, 0.0}, {-1.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
+                    {0.0, -1.0, 0.0}, {0.0, 0.0, 1.0}, {0.0, 0.0, -1.0}};
+  for (int k = 0; k < 6; k++) {
+    const D3 p = (k & 1) ? hi : ba;
+    s->bn[k][0] = ns[k].x, s->bn[k][1] = ns[k].y, s->bn[k][2] = ns[k].z;
+    s->bp[k][0] = p.x, s->bp[k][1] = p.y, s->bp[k][2] = p.z;
+    s->bd[k] = dot(ns[k], p);
+  }
+  const D3 ia = sub(ba, bw);
+  s->iloc_a[0] = ia.x, s->iloc_a[1] = ia.y, s->iloc_a[2] = ia.z;
+  s->iloc_inv[0] = 1.0 / (3.0 * bw.x);
+  s->iloc_inv[1] = 1.0 / (3.0 * bw.y);
+  s->iloc_inv[2] = 1.0 / (3.0 * bw.z);
+  // uniform grid: ~points_per_grid_cell generators per cell, at most 2^24 cells
+  double vol = 1.0;
+  for (int i = 0; i < dim; i++) vol *= ww[i];
+  const double nn = (double)std::max<int64_t>(n, 1);
+  double ppc = o.points_per_grid_cell > 0 ? o.points_per_grid_cell : 2.2;
+  double h = std::pow(vol * ppc / nn, 1.0 / dim);
+  for (;;) {
+    int64_t cells = 1;
+    for (int i = 0; i < 3; i++) {
+      int G = 1;
+      if (i < dim) G = (int)std::max(1.0, std::min(std::floor(ww[i] / h), 4096.0));
+      s->G[i] = G;
+      cells *= G;
+    }
+    if (cells <= (1ll << 24)) break;
+    h *= 1.25;
+  }
+  for (int i = 0; i < 3; i++) {
+    s->gh[i] = ww[i] / s->G[i];
+    s->ginv[i] = s->G[i] / ww[i];
+    s->geps[i] = 1e-9 * s->gh[i] + 1e-13 * (std::fabs(aa[i]) + ww[i]);
+  }
+  const double spacing = std::pow(vol / nn, 1.0 / dim);
+  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.6 : (dim == 2 ? 2.4 : 2.2));
+  s->R0 = r0 * spacing;
+  return MV_OK;
+}
+
+}  // namespace mv
+
 using namespace mv;
 
 namespace {
@@ -123,94 +206,6 @@ int ensure(mv_context* ctx, DevBuf& b, size_t bytes) {
 template <class T>
 T* P(DevBuf& b) {
   return static_cast<T*>(b.p);
-}
-
-struct Setup {
-  double anchor[3], width[3];
-  int dim, periodic;
-  int G[3];
-  double gh[3], ginv[3], geps[3];
-  double R0;
-  double bn[6][3], bp[6][3], bd[6];
-  double iloc_a[3], iloc_inv[3];
-};
-
-// voronoi.rs:200-210 + boundary.rs:14-47 + the grid resolution.
-int make_setup(int64_t n, const double* anchor, const double* width, int dim, int periodic,
-               const mv_options& o, Setup* s) {
-  if (dim < 1 || dim > 3) return MV_ERR_ARG;
-  D3 a = {anchor[0], anchor[1], anchor[2]};
-  D3 w = {width[0], width[1], width[2]};
-  if (dim == 1) {
-    a.y = -0.5;
-    w.y = 1.0;
-  }
-  if (dim == 1 || dim == 2) {
-    a.z = -0.5;
-    w.z = 1.0;
-  }
-  const double aa[3] = {a.x, a.y, a.z}, ww[3] = {w.x, w.y, w.z};
-  for (int i = 0; i < 3; i++) {
-    if (!std::isfinite(aa[i]) || !std::isfinite(ww[i]) || !(ww[i] > 0.0)) return MV_ERR_ARG;
-    s->anchor[i] = aa[i];
-    s->width[i] = ww[i];
-  }
-  s->dim = dim;
-  s->periodic = periodic ? 1 : 0;
-  // SimulationBoundary::cuboid
-  D3 ba = a, bw = w;
-  if (periodic) {
-    ba.x -= bw.x;
-    bw.x *= 3.0;
-    if (dim >= 2) {
-      ba.y -= bw.y;
-      bw.y *= 3.0;
-    }
-    if (dim == 3) {
-      ba.z -= bw.z;
-      bw.z *= 3.0;
-    }
-  }
-  const D3 hi = add(ba, bw);
-  const D3 ns[6] = {{1.0, 0.0, 0.0}, {-1.0, 0.0, 0.0}, {0.0, 1.0, 0.0},
-                    {0.0, -1.0, 0.0}, {0.0, 0.0, 1.0}, {0.0, 0.0, -1.0}};
-  for (int k = 0; k < 6; k++) {
-    const D3 p = (k & 1) ? hi : ba;
-    s->bn[k][0] = ns[k].x, s->bn[k][1] = ns[k].y, s->bn[k][2] = ns[k].z;
-    s->bp[k][0] = p.x, s->bp[k][1] = p.y, s->bp[k][2] = p.z;
-    s->bd[k] = dot(ns[k], p);
-  }
-  const D3 ia = sub(ba, bw);
-  s->iloc_a[0] = ia.x, s->iloc_a[1] = ia.y, s->iloc_a[2] = ia.z;
-  s->iloc_inv[0] = 1.0 / (3.0 * bw.x);
-  s->iloc_inv[1] = 1.0 / (3.0 * bw.y);
-  s->iloc_inv[2] = 1.0 / (3.0 * bw.z);
-  // uniform grid: ~points_per_grid_cell generators per cell, at most 2^24 cells
-  double vol = 1.0;
-  for (int i = 0; i < dim; i++) vol *= ww[i];
-  const double nn = (double)std::max<int64_t>(n, 1);
-  double ppc = o.points_per_grid_cell > 0 ? o.points_per_grid_cell : 2.2;
-  double h = std::pow(vol * ppc / nn, 1.0 / dim);
-  for (;;) {
-    int64_t cells = 1;
-    for (int i = 0; i < 3; i++) {
-      int G = 1;
-      if (i < dim) G = (int)std::max(1.0, std::min(std::floor(ww[i] / h), 4096.0));
-      s->G[i] = G;
-      cells *= G;
-    }
-    if (cells <= (1ll << 24)) break;
-    h *= 1.25;
-  }
-  for (int i = 0; i < 3; i++) {
-    s->gh[i] = ww[i] / s->G[i];
-    s->ginv[i] = s->G[i] / ww[i];
-    s->geps[i] = 1e-9 * s->gh[i] + 1e-13 * (std::fabs(aa[i]) + ww[i]);
-  }
-  const double spacing = std::pow(vol / nn, 1.0 / dim);
-  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.6 : (dim == 2 ? 2.4 : 2.2));
-  s->R0 = r0 * spacing;
-  return MV_OK;
 }
 
 double face_ratio(int dim, int face_mode) {

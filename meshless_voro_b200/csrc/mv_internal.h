@@ -104,4 +104,22 @@ struct Job {
   unsigned long long* stats;  // [ST_COUNT]
 };
 
+// Normalised simulation volume, boundary planes (boundary.rs:14-47), uniform grid and
+// first shell radius of one tessellation (mv_api.cu).
+struct Setup {
+  double anchor[3], width[3];
+  int dim, periodic;
+  int G[3];
+  double gh[3], ginv[3], geps[3];
+  double R0;
+  double bn[6][3], bp[6][3], bd[6];
+  double iloc_a[3], iloc_inv[3];
+};
+
+}  // namespace mv
+
+struct mv_options;
+namespace mv {
+int make_setup(int64_t n, const double* anchor, const double* width, int dim, int periodic,
+               const mv_options& o, Setup* s);
 }  // namespace mv
