@@ -30,6 +30,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "3D Voronoi cells/s on 1 B200: FP32-filtered batched vs plain FP64, exact topology"
 HBM_PEAK_FALLBACK = 6650.0
+# DRAM bytes (read + write) per cell of the cell kernel, from one ncu capture of the
+# 64^3 periodic Poisson case (profiles/cells_kernel_poisson64.md); traffic grows in
+# proportion to the cells, so a launch's traffic is this figure times its cells.
+CELLS_KERNEL_DRAM_BYTES_PER_CELL = 647.8
 # algorithmic bytes (generator read + cell outputs + owned faces + CSR entries)
 BYTES_GEN, BYTES_CELL, BYTES_FACE, BYTES_CONN = 24, 40, 68, 4
 
@@ -139,32 +143,30 @@ class ClockSampler:
 
 def cpu_baseline(w, budget_s=12.0, threads=None):
     """The oracle (C++ restatement of the reference algorithm) with OpenMP on all host
-    cores, on a random sample of the workload's cells; extrapolated to the full set."""
+    cores on a prefix of the workload's cells (cell order is spatially random for the
+    Poisson workloads), extrapolated to all cells."""
     from oracle import oracle as O
     g, n = w["generators"], len(w["generators"])
     threads = threads or os.cpu_count()
-    rng = np.random.default_rng(99)
     kw = dict(dim=w["dimensionality"], periodic=w["periodic"], nthreads=threads,
               flags=O.NO_CSR)
-    t0 = time.perf_counter()
-    O.build(g, w["anchor"], w["width"], mask=np.zeros(n, dtype=bool), **kw)
-    t_fixed = time.perf_counter() - t0            # grid build + flatten (serial)
-    m = min(n, 20000)
-    mask = np.zeros(n, dtype=bool)
-    mask[rng.choice(n, m, replace=False)] = True
-    t0 = time.perf_counter()
-    O.build(g, w["anchor"], w["width"], mask=mask, **kw)
-    rate = m / max(time.perf_counter() - t0 - t_fixed, 1e-6)
+
+    def run(m):
+        mask = np.zeros(n, dtype=bool)
+        mask[:m] = True
+        t0 = time.perf_counter()
+        r = O.build(g, w["anchor"], w["width"], mask=mask, **kw)
+        assert r.status == 0
+        return time.perf_counter() - t0
+
+    t_fixed = min(run(0), run(0))        # grid build + flatten (serial), no cells
+    m = min(n, 200000)
+    rate = m / max(run(m) - t_fixed, 1e-3)
     m = int(min(n, max(m, rate * budget_s)))
-    mask[:] = False
-    mask[rng.choice(n, m, replace=False)] = True
-    t0 = time.perf_counter()
-    r = O.build(g, w["anchor"], w["width"], mask=mask, **kw)
-    t_cells = time.perf_counter() - t0 - t_fixed
-    assert r.status == 0
+    t_cells = max(run(m) - t_fixed, 1e-6)
     full = t_fixed + t_cells * n / m
     return {"value": n / full, "unit": "cells/s", "cores": threads, "kind": "port",
-            "sample": f"{m} random cells of the same {n}-generator workload "
+            "sample": f"first {m} of the {n} cells of the same workload "
                       f"({t_cells:.1f} s of cell work + {t_fixed:.1f} s serial grid build, "
                       f"extrapolated to all cells)"}
 
@@ -312,8 +314,9 @@ def main():
     peak, peak_kind = measured_peaks()
     alg_bytes = BYTES_GEN * n + BYTES_CELL * n + BYTES_FACE * F + BYTES_CONN * Cn
     achieved = alg_bytes / (cells_ms * 1e-3) / 1e9
+    traffic = CELLS_KERNEL_DRAM_BYTES_PER_CELL * n if args.workload.startswith("poisson") else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "mv::cells_kernel", "alg_bytes_per_launch": alg_bytes,
                 "kernel_ms": cells_ms}
 
