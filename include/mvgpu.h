@@ -50,12 +50,23 @@ enum {
 /* ---- dimensionality (voronoi.rs:31-40) ---- */
 enum { MV_DIM_1 = 1, MV_DIM_2 = 2, MV_DIM_3 = 3 };
 
+/* ---- how the cells are built (results are identical either way) ---- */
+enum {
+  MV_PIPELINE_AUTO = 0,    /* staged for large builds, fused for small ones          */
+  MV_PIPELINE_STAGED = 1,  /* per chunk: shell, clip and integral kernels; cells that
+                              need more than the first neighbour shell are rebuilt by
+                              the fused kernel                                        */
+  MV_PIPELINE_FUSED = 2    /* one kernel builds each cell from start to finish        */
+};
+
 typedef struct mv_options {
   int precision;                 /* MV_PRECISION_*                                   */
   int face_mode;                 /* MV_FACES_*                                       */
   double points_per_grid_cell;   /* 0: library default                               */
   double initial_radius;         /* first neighbour shell, in mean spacings; 0: default */
   void* stream;                  /* cudaStream_t to run on; NULL: the context stream */
+  int pipeline;                  /* MV_PIPELINE_*                                    */
+  int chunk_cells;               /* staged pipeline: cells per chunk; 0: default     */
 } mv_options;
 
 /* Per-build counters (escalations and retries). */
@@ -68,6 +79,7 @@ typedef struct mv_build_stats {
   int64_t extra_shells;          /* neighbour-shell expansions beyond the first      */
   int64_t overflow_cells;        /* cells re-run in the large capacity tier          */
   int64_t serial_rings;          /* rings rebuilt by the serial fallback             */
+  int64_t staged_retries;        /* staged pipeline: cells rebuilt by the fused kernel */
   int64_t device_bytes;          /* device workspace held by the context             */
   int64_t kernel_launches;       /* library kernels launched by the build            */
   double ms_grid;                /* device time: generator prep + uniform grid       */

@@ -27,6 +27,10 @@ MV_PRECISION_FILTERED = 1
 MV_FACES_OWNED = 0
 MV_FACES_ALL = 1
 
+MV_PIPELINE_AUTO = 0
+MV_PIPELINE_STAGED = 1
+MV_PIPELINE_FUSED = 2
+
 NO_SHIFT = 13
 
 # every symbol include/mvgpu.h declares
@@ -41,13 +45,14 @@ EXPORTED = (
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("face_mode", C.c_int),
                 ("points_per_grid_cell", C.c_double), ("initial_radius", C.c_double),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("pipeline", C.c_int), ("chunk_cells", C.c_int)]
 
 
 class BuildStats(C.Structure):
     _fields_ = [(name, C.c_int64) for name in (
         "cells_built", "neighbours_clipped", "planes_added", "f32_undecided", "exact_tests",
-        "extra_shells", "overflow_cells", "serial_rings", "device_bytes", "kernel_launches")] + [
+        "extra_shells", "overflow_cells", "serial_rings", "staged_retries", "device_bytes",
+        "kernel_launches")] + [
         (name, C.c_double) for name in ("ms_grid", "ms_cells", "ms_finalize")]
 
     def as_dict(self):

@@ -17,8 +17,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libmvgpu.so")
 
-SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu"]
-HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h"]
+SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu", "mv_staged.cu"]
+HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h", "mv_cell_common.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = [

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/mvgpu.h"
 #include "mv_geom.cuh"
@@ -22,6 +23,11 @@ namespace mv {
 cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
 int cells_blocks_per_sm_fast(int precision);
 int cells_blocks_per_sm_large(int precision);
+// mv_staged.cu
+cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st);
+int stage_blocks_per_sm(int kernel, int precision);
+int stage_list_stride();
+int64_t stage_record_words(int np, int nv);
 // mv_grid.cu
 void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
                  double* ext, int* bad, cudaStream_t st);
@@ -140,6 +146,8 @@ struct Workspace {
   DevBuf f_left, f_right, f_area, f_cen, f_nrm, f_code;
   DevBuf ovf_a, ovf_b;
   DevBuf counters;
+  // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
+  DevBuf cand, cand_info, rec_off, rec, retry, stage_ctr;
 };
 
 }  // namespace
@@ -147,14 +155,17 @@ struct Workspace {
 struct mv_context {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[10] = {};
   int sm_count = 0;
   int bps_fast[2] = {0, 0};
   int bps_large[2] = {0, 0};
+  int bps_stage[3][2] = {};  // shell, clip, integral kernels by precision
+  double rec_words_hint = 0.0;  // record words per cell the last staged build needed
   Workspace ws;
   size_t dev_bytes = 0;
   double face_ratio_hint = 0.0;  // faces per cell needed by the last build
   bool large_ran = false;
+  bool retry_ran = false;
   mv_build_stats last{};
   // pinned host arena for mv_context_build
   void* host = nullptr;
@@ -214,6 +225,78 @@ double face_ratio(int dim, int face_mode) {
   return 2.5;
 }
 
+// The staged pipeline runs for builds large enough to fill the GPU with chunks; the
+// candidate list packs a sorted position with a shift code into 32 bits.
+bool use_staged(const mv_options& o, int64_t n) {
+  if (n <= 0 || n >= (int64_t)(0xffffffffu / 27u)) return false;
+  if (o.pipeline == MV_PIPELINE_STAGED) return true;
+  if (o.pipeline == MV_PIPELINE_FUSED) return false;
+  return n >= 65536;
+}
+
+int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224 : 128); }
+
+// Shell, clip and integral kernels over chunks of cells in processing (grid) order.
+// Cells the first shell does not decide are appended to the retry list; *n_retry
+// receives their number.
+int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& o, int64_t n,
+               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry) {
+  Workspace& W = ctx->ws;
+  const int64_t chunk = std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
+  const int64_t nchunks = (n + chunk - 1) / chunk;
+  const int stride = stage_list_stride();
+  int64_t wpc = std::max<int64_t>(record_words_per_cell(s.dim), (int64_t)ctx->rec_words_hint);
+  wpc = std::min<int64_t>(wpc, stage_record_words(64, 64));
+  const int64_t rec_cap = chunk * wpc;
+  const size_t ctr_words = 1 + 3 * (size_t)nchunks;
+  int e = 0;
+  e |= ensure(ctx, W.cand, 4 * (size_t)chunk * stride);
+  e |= ensure(ctx, W.cand_info, 4 * (size_t)chunk);
+  e |= ensure(ctx, W.rec_off, 8 * (size_t)chunk);
+  e |= ensure(ctx, W.rec, 8 * (size_t)rec_cap);
+  e |= ensure(ctx, W.retry, 4 * (size_t)n);
+  e |= ensure(ctx, W.stage_ctr, 8 * ctr_words);
+  if (e) return MV_ERR_OOM;
+  unsigned long long* ctr = P<unsigned long long>(W.stage_ctr);
+  MV_CUDA(cudaMemsetAsync(ctr, 0, 8 * ctr_words, st));
+  StageJob SJ;
+  std::memset(&SJ, 0, sizeof(SJ));
+  SJ.cstride = stride;
+  SJ.cand = P<uint32_t>(W.cand);
+  SJ.info = P<int32_t>(W.cand_info);
+  SJ.rec_off = P<int64_t>(W.rec_off);
+  SJ.rec = P<double>(W.rec);
+  SJ.rec_cap = rec_cap;
+  SJ.retry_list = P<int32_t>(W.retry);
+  SJ.retry_count = reinterpret_cast<unsigned int*>(ctr);
+  for (int64_t c = 0; c < nchunks; c++) {
+    SJ.item0 = (int32_t)(c * chunk);
+    SJ.nitems = (int32_t)std::min<int64_t>(chunk, n - c * chunk);
+    SJ.work = reinterpret_cast<unsigned int*>(ctr + 1 + 3 * c);
+    SJ.rec_counter = ctr + 1 + 3 * c + 2;
+    const int64_t warps_needed = SJ.nitems;
+    for (int k = 0; k < 3; k++) {
+      const int wpb = 4;  // every stage kernel runs 4 warps per block
+      int64_t blocks = (int64_t)ctx->sm_count * std::max(1, ctx->bps_stage[k][pi]);
+      blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
+      MV_CUDA(launch_stage(k, J, SJ, (int)std::max<int64_t>(1, blocks), st));
+      (*launches)++;
+    }
+  }
+  std::vector<unsigned long long> h(ctr_words);
+  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * ctr_words, cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaStreamSynchronize(st));
+  *n_retry = (int64_t)(h[0] & 0xffffffffull);
+  // size the record buffer of the next build by what this one asked for
+  double need = 0.0;
+  for (int64_t c = 0; c < nchunks; c++) {
+    const int64_t items = std::min<int64_t>(chunk, n - c * chunk);
+    need = std::max(need, (double)h[1 + 3 * c + 2] / (double)std::max<int64_t>(items, 1));
+  }
+  if (need * 1.1 > (double)wpc) ctx->rec_words_hint = need * 1.2;
+  return MV_OK;
+}
+
 int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mask, int64_t n,
                       const double* anchor, const double* width, int dim, int periodic,
                       const mv_options* opts_in, mv_device_voronoi* out) {
@@ -224,6 +307,8 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   if (n >= (int64_t)(0xffffffffu / 27u)) return MV_ERR_ARG;  // neighbour tie key range
   if (o.precision != MV_PRECISION_FP64 && o.precision != MV_PRECISION_FILTERED) return MV_ERR_ARG;
   if (o.face_mode != MV_FACES_OWNED && o.face_mode != MV_FACES_ALL) return MV_ERR_ARG;
+  if (o.pipeline < MV_PIPELINE_AUTO || o.pipeline > MV_PIPELINE_FUSED || o.chunk_cells < 0)
+    return MV_ERR_ARG;
   Setup s;
   int rc = make_setup(n, anchor, width, dim, periodic, o, &s);
   if (rc) return rc;
@@ -356,13 +441,37 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.status = C->status;
     J.stats = C->stats;
     const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
+    const bool staged = use_staged(o, n);
+    bool retry_ran = false;
+    int64_t n_retry = 0;
     MV_CUDA(cudaEventRecord(ctx->ev[1], st));
-    if (n > 0) {
-      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
-      MV_CUDA(launch_cells(J, false, blocks, st));
-      launches++;
+    if (n > 0 && staged) {
+      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry);
+      if (rc2) return rc2;
+      MV_CUDA(cudaEventRecord(ctx->ev[2], st));
+      if (n_retry > 0) {
+        // cells the first shell did not decide: the fused kernel builds them
+        Job Rj = J;
+        Rj.order = P<int32_t>(W.retry);
+        Rj.n_order = (int32_t)n_retry;
+        int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+        blocks = (int)std::min<int64_t>(blocks, (n_retry + 3) / 4);
+        MV_CUDA(cudaEventRecord(ctx->ev[7], st));
+        MV_CUDA(launch_cells(Rj, false, blocks, st));
+        MV_CUDA(cudaEventRecord(ctx->ev[8], st));
+        launches++;
+        retry_ran = true;
+      }
+    } else {
+      if (n > 0) {
+        int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+        MV_CUDA(launch_cells(J, false, blocks, st));
+        launches++;
+      }
+      MV_CUDA(cudaEventRecord(ctx->ev[2], st));
     }
-    MV_CUDA(cudaEventRecord(ctx->ev[2], st));
+    ctx->retry_ran = retry_ran;
+    stats.staged_retries = n_retry;
     bool large_ran = false;
     DevCounters hc;
     MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
@@ -455,13 +564,14 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   stats.device_bytes = (int64_t)ctx->dev_bytes;
   stats.kernel_launches = launches;
   {
-    float t01 = 0.f, t12 = 0.f, t34 = 0.f, t56 = 0.f;
+    float t01 = 0.f, t12 = 0.f, t34 = 0.f, t56 = 0.f, t78 = 0.f;
     cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&t12, ctx->ev[1], ctx->ev[2]);
     if (ctx->large_ran) cudaEventElapsedTime(&t34, ctx->ev[3], ctx->ev[4]);
+    if (ctx->retry_ran) cudaEventElapsedTime(&t78, ctx->ev[7], ctx->ev[8]);
     cudaEventElapsedTime(&t56, ctx->ev[5], ctx->ev[6]);
     stats.ms_grid = t01;
-    stats.ms_cells = t12 + t34;
+    stats.ms_cells = t12 + t34 + t78;
     stats.ms_finalize = t56;
   }
   ctx->last = stats;
@@ -702,7 +812,7 @@ int mv_context_create(int device, mv_context** out) {
   ctx->device = dev;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, dev);
-  for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+  for (int i = 0; i < 10 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
   if (e != cudaSuccess) {
     delete ctx;
     return cuda_status(e);
@@ -710,6 +820,7 @@ int mv_context_create(int device, mv_context** out) {
   for (int p = 0; p < 2; p++) {
     ctx->bps_fast[p] = cells_blocks_per_sm_fast(p);
     ctx->bps_large[p] = cells_blocks_per_sm_large(p);
+    for (int k = 0; k < 3; k++) ctx->bps_stage[k][p] = stage_blocks_per_sm(k, p);
   }
   if (cudaGetLastError() != cudaSuccess || ctx->bps_fast[0] <= 0 || ctx->bps_fast[1] <= 0) {
     cudaStreamDestroy(ctx->stream);
@@ -729,7 +840,7 @@ void mv_context_destroy(mv_context* ctx) {
   for (size_t i = 0; i < nb; i++)
     if (bufs[i].p) cudaFree(bufs[i].p);
   if (ctx->host) cudaFreeHost(ctx->host);
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 10; i++)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -1,0 +1,707 @@
+// mv_cell_common.cuh -- device building blocks shared by the cell kernels.
+//
+// The fused cell kernel (mv_cells.cu) and the staged shell / clip / integral kernels
+// (mv_staged.cu) are built from these pieces:
+//   * the nearest-first neighbour shell (rtree_nn.rs:10-240) gathered from the
+//     uniform grid and sorted by (f64 squared distance, original index, shift code);
+//   * the exact clip decision (half_space.rs:40-47, boundary.rs:49-64,
+//     geometry.rs:271-314), Vertex::from_dual (convex_cell.rs:28-48) and the ring of a
+//     clip (compute_boundary + SimpleCycle, convex_cell.rs:421-441, simple_cycle.rs);
+//   * the cell and face integrals (convex_cell.rs:131-187, voronoi_cell.rs:40-100,
+//     integrals.rs) over a read-only view of a finished cell.
+// Cell-state functions are templates over the shared-memory layout `SM`, which
+// provides the plane arrays pnx/pny/pnz/pd/ppx/ppy/ppz/pright/pcode/rptr and the
+// vertex arrays vx/vy/vz/vr2/f4/vd0/vd1/vd2/ord/ea/eb under those names (f4 holds the
+// f32 offset v - x of the filter; ord is 4-byte aligned).
+#pragma once
+#include <cstdint>
+
+#include "../../include/mvgpu.h"
+#include "mv_exact.cuh"
+#include "mv_geom.cuh"
+#include "mv_internal.h"
+
+namespace mv {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <int VMAX_, int PMAX_, int CMAX_, int KMAX_, typename PIdx_, int MINB_>
+struct Tier {
+  static constexpr int MINB = MINB_;  // min resident blocks per SM (register budget)
+  static constexpr int VMAX = VMAX_;  // vertices
+  static constexpr int PMAX = PMAX_;  // clipping planes
+  static constexpr int CMAX = CMAX_;  // neighbour-shell entries
+  static constexpr int KMAX = KMAX_;  // neighbours set up per batch
+  static constexpr int NW = VMAX / 32;
+  using PIdx = PIdx_;
+  static constexpr unsigned NONE = (unsigned)(PIdx)(~0u);
+  static_assert(VMAX % 32 == 0 && PMAX % 32 == 0 && CMAX % 32 == 0, "tier sizes");
+  static_assert(PMAX < (int)NONE && VMAX < (int)NONE, "index type too small");
+  static_assert(KMAX <= 32, "batch is set up by one lane per neighbour");
+};
+
+// ------------------------------------------------------------ small helpers --
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  *total = __shfl_sync(FULL, x, 31);
+  return x - v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// Largest non-negative double over the warp: non-negative binary64 values order like
+// their bit patterns, so two 32-bit warp reductions give the exact maximum.
+__device__ __forceinline__ double warp_max_nonneg(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)b;
+  const unsigned mhi = __reduce_max_sync(FULL, hi);
+  const unsigned mlo = __reduce_max_sync(FULL, hi == mhi ? lo : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+}
+
+__device__ __forceinline__ D3 shfl_d3(D3 v, int src) {
+  return {__shfl_sync(FULL, v.x, src), __shfl_sync(FULL, v.y, src), __shfl_sync(FULL, v.z, src)};
+}
+
+template <int NW>
+__device__ __forceinline__ int rank_below(const unsigned (&m)[NW], int p) {
+  int r = 0;
+#pragma unroll
+  for (int w = 0; w < NW; w++) {
+    if (w < (p >> 5))
+      r += __popc(m[w]);
+    else if (w == (p >> 5))
+      r += __popc(m[w] & ((1u << (p & 31)) - 1u));
+  }
+  return r;
+}
+
+// position of the s-th (1-based) set bit
+template <int NW>
+__device__ __forceinline__ int select_bit(const unsigned (&m)[NW], int s) {
+#pragma unroll
+  for (int w = 0; w < NW; w++) {
+    int c = __popc(m[w]);
+    if (s <= c) return 32 * w + (int)__fns(m[w], 0, s);
+    s -= c;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ unsigned valid_bits(int nv, int w) {
+  const int lim = nv - 32 * w;
+  return lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
+}
+
+__device__ __forceinline__ void iloc(const Job& J, D3 l, int64_t out[3]) {
+  const uint64_t mask = 0xFFFFFFFFFFFFFull;
+  double c0 = 1.0 + (l.x - J.iloc_a[0]) * J.iloc_inv[0];
+  double c1 = 1.0 + (l.y - J.iloc_a[1]) * J.iloc_inv[1];
+  double c2 = 1.0 + (l.z - J.iloc_a[2]) * J.iloc_inv[2];
+  out[0] = (int64_t)((uint64_t)__double_as_longlong(c0) & mask);
+  out[1] = (int64_t)((uint64_t)__double_as_longlong(c1) & mask);
+  out[2] = (int64_t)((uint64_t)__double_as_longlong(c2) & mask);
+}
+
+__device__ __forceinline__ D3 load_gen(const Job& J, int orig) {
+  const double* g = J.gen + 3 * (int64_t)orig;
+  return {__ldg(g), __ldg(g + 1), __ldg(g + 2)};
+}
+
+// HalfSpace::right_loc (half_space.rs:53-65)
+template <class SM>
+__device__ __forceinline__ D3 right_loc(const Job& J, const SM& S, int k, D3 x) {
+  int r = S.pright[k];
+  if (r >= 0) {
+    D3 l = load_gen(J, r);
+    int code = S.pcode[k];
+    if (code != 13) l = add(l, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+    return l;
+  }
+  D3 pr = plane_project({S.pnx[k], S.pny[k], S.pnz[k]}, {S.ppx[k], S.ppy[k], S.ppz[k]}, x);
+  return sub(scale(2.0, pr), x);
+}
+
+// Exact decision of clip_by_plane for an undecided vertex in slot `s`
+// (convex_cell.rs:370-382).
+template <class SM>
+__device__ __noinline__ int exact_clip(const Job& J, const SM& S, int s, D3 x, D3 ngb) {
+  int64_t A[3], B[3], C[3], Dd[3], W[3];
+  iloc(J, x, A);
+  iloc(J, right_loc(J, S, S.vd0[s], x), B);
+  iloc(J, right_loc(J, S, S.vd1[s], x), C);
+  iloc(J, right_loc(J, S, S.vd2[s], x), Dd);
+  iloc(J, ngb, W);
+  return in_sphere_exact_sign(A, B, C, Dd, W);
+}
+
+// Vertex::from_dual (convex_cell.rs:28-48) into slot `slot`; *r2 receives the
+// vertex's squared distance to the generator.
+template <class PIdx, class SM>
+__device__ __forceinline__ bool make_vertex(SM& S, int slot, int i, int j, int k, D3 x, int dim,
+                                            double* r2) {
+  D3 loc;
+  bool ok = intersect3({S.pnx[i], S.pny[i], S.pnz[i]}, S.pd[i], {S.pnx[j], S.pny[j], S.pnz[j]},
+                       S.pd[j], {S.pnx[k], S.pny[k], S.pnz[k]}, S.pd[k], &loc);
+  if (!ok) return false;
+  D3 dl = loc;
+  if (dim == 1) dl = {loc.x, 0.0, 0.0};
+  if (dim == 2) dl = {loc.x, loc.y, 0.0};
+  D3 r = sub(x, dl);
+  const double rr = dot(r, r);
+  S.vx[slot] = loc.x;
+  S.vy[slot] = loc.y;
+  S.vz[slot] = loc.z;
+  S.vr2[slot] = rr;
+  S.f4[slot] = make_float4(__double2float_rn(loc.x - x.x), __double2float_rn(loc.y - x.y),
+                           __double2float_rn(loc.z - x.z), 0.f);
+  S.vd0[slot] = (PIdx)i;
+  S.vd1[slot] = (PIdx)j;
+  S.vd2[slot] = (PIdx)k;
+  *r2 = rr;
+  return true;
+}
+
+// Vertex duals of the initial cuboid (convex_cell.rs:298-307), one vertex per lane.
+__device__ __forceinline__ void cuboid_duals(int lane, int* i0, int* i1, int* i2) {
+  switch (lane) {
+    case 0: *i0 = 2, *i1 = 5, *i2 = 0; break;
+    case 1: *i0 = 5, *i1 = 3, *i2 = 0; break;
+    case 2: *i0 = 1, *i1 = 5, *i2 = 2; break;
+    case 3: *i0 = 5, *i1 = 1, *i2 = 3; break;
+    case 4: *i0 = 4, *i1 = 2, *i2 = 0; break;
+    case 5: *i0 = 4, *i1 = 0, *i2 = 3; break;
+    case 6: *i0 = 2, *i1 = 4, *i2 = 1; break;
+    default: *i0 = 4, *i1 = 3, *i2 = 1; break;
+  }
+}
+
+// Bound on |v - x| over the cell's vertices for the f32 filter: r2 omits the
+// extruded dimensions, whose vertex coordinates are +-0.5.
+__device__ __forceinline__ double amax_of(double max_r2, int dim) {
+  return sqrt((max_r2 + 0.26 * (3 - dim)) * (1.0 + 1e-9)) * (1.0 + 1e-9);
+}
+
+enum CellResult {
+  CELL_DONE = 0,
+  CELL_OVERFLOW = 1,
+  CELL_ERROR = 2,
+  CELL_FACE_OVERFLOW = 3,
+  CELL_RETRY = 4  // staged path: the cell needs the fused kernel (more neighbours)
+};
+
+// Event counts of one cell, kept in warp-uniform registers (a lane-0 branch inside
+// the clip loop would split the warp) and flushed once per cell.
+struct CellCount {
+  unsigned c[ST_COUNT];
+};
+#define WCNT(CC, slot, v) ((CC).c[slot] += (unsigned)(v))
+
+// ------------------------------------------------------------- neighbour shell --
+template <int CMAX>
+struct ShellBuf {
+  unsigned long long key[CMAX];  // f64 squared distance bits
+  uint32_t tie[CMAX];            // original index * 27 + shift code
+  int32_t cpos[CMAX];            // grid-sorted position of the generator
+  int32_t sstart[96];
+  int32_t spref[97];
+  uint8_t scode[96];
+};
+
+// Gathers every stream element (generator, periodic image) with lo2 <= d2 < R*R into
+// B (unsorted) and returns how many there are (may exceed CMAX).  *exhausted is set
+// when the enumerated cells cover every image and none lies beyond R, i.e. the stream
+// ends with this shell.  d2 is the reference's squared distance:
+// (g - q).length_squared() for nn_iter (rstar) and |(q + s) - g|^2 for
+// wrapping_nn_iter (rtree_nn.rs:138-146).
+template <int CMAX>
+__device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
+                                         double lo2, const double* ext, bool* exhausted) {
+  const double xa[3] = {x.x, x.y, x.z};
+  int lo[3], hi[3];
+  bool all = true;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    int G = J.G[i];
+    bool wrap = J.periodic && i < J.dim;
+    int umin = wrap ? -G : 0, umax = wrap ? 2 * G - 1 : G - 1;
+    double fl = floor((xa[i] - R - J.ga[i]) * J.ginv[i]) - 1.0;
+    double fh = floor((xa[i] + R - J.ga[i]) * J.ginv[i]) + 1.0;
+    lo[i] = fl < (double)umin ? umin : (int)fl;
+    hi[i] = fh > (double)umax ? umax : (int)fh;
+    if (lo[i] > umin || hi[i] < umax) all = false;
+  }
+  const double R2 = R * R;
+  const double R2v = R2 * (1.0 + 1e-9);
+  int beyond = 0;
+  const int ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+  const int nrows = ny * nz;
+  int count = 0;
+
+  // box-distance of unwrapped grid coordinate u along axis i
+  auto box_d = [&](int i, int u) -> double {
+    int G = J.G[i];
+    bool wrap = J.periodic && i < J.dim;
+    int m = u < 0 ? -1 : (u >= G ? 1 : 0);
+    int c = u - m * G;
+    double blo = J.ga[i] + c * J.gh[i], bhi = J.ga[i] + (c + 1) * J.gh[i];
+    if (c == 0) blo = wrap ? fmin(blo, ext[i]) : -__longlong_as_double(0x7ff0000000000000ll);
+    if (c == G - 1) bhi = wrap ? fmax(bhi, ext[3 + i]) : __longlong_as_double(0x7ff0000000000000ll);
+    blo += m * J.gw[i] - J.geps[i];
+    bhi += m * J.gw[i] + J.geps[i];
+    return xa[i] < blo ? blo - xa[i] : (xa[i] > bhi ? xa[i] - bhi : 0.0);
+  };
+
+  for (int row0 = 0; row0 < nrows; row0 += 32) {
+    const int row = row0 + lane;
+    int nseg = 0;
+    int32_t s0a = 0, s0b = 0, s0c = 0, sla = 0, slb = 0, slc = 0;
+    int sca = 0, scb = 0, scc = 0;
+    if (row < nrows) {
+      const int uy = lo[1] + row % ny, uz = lo[2] + row / ny;
+      const double dy = box_d(1, uy), dz = box_d(2, uz);
+      const double byz2 = dy * dy + dz * dz;
+      if (all || byz2 < R2v) {
+        int first = 1 << 30, last = -(1 << 30);
+        for (int ux = lo[0]; ux <= hi[0]; ux++) {
+          double dx = box_d(0, ux);
+          if (all || dx * dx + byz2 < R2v) {
+            first = min(first, ux);
+            last = max(last, ux);
+          }
+        }
+        const int Gx = J.G[0], Gy = J.G[1], Gz = J.G[2];
+        const int my = uy < 0 ? -1 : (uy >= Gy ? 1 : 0);
+        const int mz = uz < 0 ? -1 : (uz >= Gz ? 1 : 0);
+        const int cy = uy - my * Gy, cz = uz - mz * Gz;
+        const int64_t rowbase = (int64_t)Gx * (cy + (int64_t)Gy * cz);
+        for (int mx = -1; mx <= 1; mx++) {
+          int a = max(first, mx * Gx), b = min(last, mx * Gx + Gx - 1);
+          if (a > b) continue;
+          int c0 = a - mx * Gx, c1 = b - mx * Gx;
+          int32_t ps = __ldg(J.cell_start + rowbase + c0);
+          int32_t pe = __ldg(J.cell_start + rowbase + c1 + 1);
+          if (pe > ps) {
+            const int code = (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+            if (nseg == 0) {
+              s0a = ps, sla = pe - ps, sca = code;
+            } else if (nseg == 1) {
+              s0b = ps, slb = pe - ps, scb = code;
+            } else {
+              s0c = ps, slc = pe - ps, scc = code;
+            }
+            nseg++;
+          }
+        }
+      }
+    }
+    int nsegs_total;
+    const int segoff = warp_excl_scan(nseg, lane, &nsegs_total);
+    const int mylen = sla + slb + slc;
+    int total;
+    const int lenoff = warp_excl_scan(mylen, lane, &total);
+    if (nseg > 0) {
+      B.sstart[segoff] = s0a, B.spref[segoff] = lenoff, B.scode[segoff] = (uint8_t)sca;
+    }
+    if (nseg > 1) {
+      B.sstart[segoff + 1] = s0b, B.spref[segoff + 1] = lenoff + sla;
+      B.scode[segoff + 1] = (uint8_t)scb;
+    }
+    if (nseg > 2) {
+      B.sstart[segoff + 2] = s0c, B.spref[segoff + 2] = lenoff + sla + slb;
+      B.scode[segoff + 2] = (uint8_t)scc;
+    }
+    __syncwarp();
+    for (int t0 = 0; t0 < total; t0 += 32) {
+      const int t = t0 + lane;
+      bool keep = false;
+      double d2 = 0.0;
+      uint32_t tie = 0;
+      int s = 0;
+      if (t < total) {
+        int a = 0, b = nsegs_total - 1;
+        while (a < b) {
+          int mid = (a + b + 1) >> 1;
+          if (B.spref[mid] <= t)
+            a = mid;
+          else
+            b = mid - 1;
+        }
+        s = B.sstart[a] + (t - B.spref[a]);
+        const int code = B.scode[a];
+        const double px = __ldg(J.sx + s), py = __ldg(J.sy + s), pz = __ldg(J.sz + s);
+        const int orig = __ldg(J.sid + s);
+        if (J.periodic) {
+          const double ddx = (x.x + J.qshift[code][0]) - px;
+          const double ddy = (x.y + J.qshift[code][1]) - py;
+          const double ddz = (x.z + J.qshift[code][2]) - pz;
+          d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        } else {
+          D3 dd = sub(D3{px, py, pz}, x);
+          d2 = dot(dd, dd);
+        }
+        keep = (d2 >= lo2) && (d2 < R2);
+        beyond += (d2 >= R2);
+        tie = (uint32_t)orig * 27u + (uint32_t)code;
+      }
+      const unsigned bal = __ballot_sync(FULL, keep);
+      const int pos = count + __popc(bal & lanemask_lt());
+      if (keep && pos < CMAX) {
+        B.key[pos] = (unsigned long long)__double_as_longlong(d2);
+        B.tie[pos] = tie;
+        B.cpos[pos] = s;
+      }
+      count += __popc(bal);
+    }
+    __syncwarp();
+  }
+  *exhausted = all && !__any_sync(FULL, beyond > 0);
+  return count;
+}
+
+// Bitonic sort of the shell [0, n) by (key, tie) ascending, carrying cpos; n <= CMAX.
+template <int CMAX>
+__device__ __noinline__ void sort_shell(ShellBuf<CMAX>& B, int lane, int n) {
+  int np2 = 32;
+  while (np2 < n) np2 <<= 1;
+  for (int i = n + lane; i < np2; i += 32) {
+    B.key[i] = ~0ull;
+    B.tie[i] = ~0u;
+    B.cpos[i] = 0;
+  }
+  __syncwarp();
+  for (int k = 2; k <= np2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < (np2 >> 1); i += 32) {
+        const int lo = 2 * j * (i / j) + (i % j);
+        const int hi = lo + j;
+        const bool asc = (lo & k) == 0;
+        const unsigned long long ka = B.key[lo], kb = B.key[hi];
+        const uint32_t ta = B.tie[lo], tb = B.tie[hi];
+        const bool gt = (ka > kb) || (ka == kb && ta > tb);
+        if (gt == asc) {
+          const int32_t pa = B.cpos[lo], pb = B.cpos[hi];
+          B.key[lo] = kb;
+          B.key[hi] = ka;
+          B.tie[lo] = tb;
+          B.tie[hi] = ta;
+          B.cpos[lo] = pb;
+          B.cpos[hi] = pa;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// -------------------------------------------------------------------- ring --
+// Serial replay of compute_boundary (convex_cell.rs:421-441) and SimpleCycle
+// (simple_cycle.rs:17-78) on lane 0 for the removed vertices at positions [nvf, nv).
+// Produces the edge list (S.ea, S.eb) and returns its length, -1 on failure, -2 when
+// the ring exceeds the tier's vertex capacity.
+template <class T, class SM>
+__device__ __noinline__ int ring_serial(SM& S, int nvf, int nv, int np) {
+  using PIdx = typename T::PIdx;
+  for (int i = 0; i < np; i++) S.rptr[i] = (PIdx)i;
+  auto contains = [&](int i) { return S.rptr[i] != (PIdx)i; };
+  const int s0 = S.ord[nvf];
+  int start = S.vd0[s0];
+  int len = 3;
+  {
+    int a = S.vd0[s0], b = S.vd1[s0], c = S.vd2[s0];
+    S.rptr[a] = (PIdx)b;
+    S.rptr[b] = (PIdx)c;
+    S.rptr[c] = (PIdx)a;
+  }
+  const int n = nv - nvf;
+  for (int i = 1; i < n; i++) {
+    int idx = i;
+    for (;;) {
+      if (idx >= n) return -1;
+      const int sl = S.ord[nvf + idx];
+      const int t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
+      const bool i0 = contains(t0), i1 = contains(t1), i2 = contains(t2);
+      bool ok = false;
+      for (int a = 0; a < 3 && !ok; a++) {
+        // rotation (ta, tb, tc) = (tri[a], tri[a+1], tri[a+2])
+        const int ta = a == 0 ? t0 : (a == 1 ? t1 : t2);
+        const int tb = a == 0 ? t1 : (a == 1 ? t2 : t0);
+        const int tc = a == 0 ? t2 : (a == 1 ? t0 : t1);
+        const bool ia = a == 0 ? i0 : (a == 1 ? i1 : i2);
+        const bool ib = a == 0 ? i1 : (a == 1 ? i2 : i0);
+        const bool ic = a == 0 ? i2 : (a == 1 ? i0 : i1);
+        if (!ia && ib && ic && S.rptr[tc] == (PIdx)tb) {
+          S.rptr[tc] = (PIdx)ta;
+          S.rptr[ta] = (PIdx)tb;
+          len += 1;
+          ok = true;
+        } else if (ia && ib && ic && S.rptr[tc] == (PIdx)tb && S.rptr[tb] == (PIdx)ta) {
+          S.rptr[tc] = (PIdx)ta;
+          S.rptr[tb] = (PIdx)tb;
+          if (start == tb) start = ta;
+          len -= 1;
+          ok = true;
+        }
+      }
+      if (ok) {
+        if (idx > i) {
+          const PIdx tmp = S.ord[nvf + i];
+          S.ord[nvf + i] = S.ord[nvf + idx];
+          S.ord[nvf + idx] = tmp;
+        }
+        break;
+      }
+      idx++;
+    }
+  }
+  if (len > T::VMAX) return -2;
+  int cur = start;
+  for (int e = 0; e < len; e++) {
+    const int nxt = S.rptr[cur];
+    S.ea[e] = (PIdx)cur;
+    S.eb[e] = (PIdx)nxt;
+    cur = nxt;
+  }
+  return len;
+}
+
+// Parallel ring: the boundary edges of the union of the removed dual triangles form
+// the same cycle the serial algorithm builds; it starts at the first removed
+// vertex's dual[0] whenever that node is still on the boundary.  Returns the edge
+// count, or -1 when the serial replay must decide.
+template <class T, class SM>
+__device__ __forceinline__ int ring_parallel(SM& S, int lane, int nvf, int nv) {
+  using PIdx = typename T::PIdx;
+  const int r = nv - nvf;
+  if (r > 32) return -1;  // large removal sets: the serial replay decides
+  int t0 = 0, t1 = 0, t2 = 0;
+  if (lane < r) {
+    const int sl = S.ord[nvf + lane];
+    t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
+    S.rptr[t0] = (PIdx)T::NONE;
+    S.rptr[t1] = (PIdx)T::NONE;
+    S.rptr[t2] = (PIdx)T::NONE;
+  }
+  __syncwarp();
+  // an edge u->w of a removed triangle is on the boundary iff no other removed
+  // triangle holds w->u
+  bool b01 = lane < r, b12 = lane < r, b20 = lane < r;
+  for (int k = 0; k < r; k++) {
+    const int a = __shfl_sync(FULL, t0, k), b = __shfl_sync(FULL, t1, k),
+              c = __shfl_sync(FULL, t2, k);
+    if (k == lane) continue;
+    b01 = b01 && !((a == t1 && b == t0) || (b == t1 && c == t0) || (c == t1 && a == t0));
+    b12 = b12 && !((a == t2 && b == t1) || (b == t2 && c == t1) || (c == t2 && a == t1));
+    b20 = b20 && !((a == t0 && b == t2) || (b == t0 && c == t2) || (c == t0 && a == t2));
+  }
+  if (b01) S.rptr[t0] = (PIdx)t1;
+  if (b12) S.rptr[t1] = (PIdx)t2;
+  if (b20) S.rptr[t2] = (PIdx)t0;
+  __syncwarp();
+  bool conflict = (b01 && S.rptr[t0] != (PIdx)t1) || (b12 && S.rptr[t1] != (PIdx)t2) ||
+                  (b20 && S.rptr[t2] != (PIdx)t0);
+  if (__any_sync(FULL, conflict)) return -1;
+  const int E = __popc(__ballot_sync(FULL, b01)) + __popc(__ballot_sync(FULL, b12)) +
+                __popc(__ballot_sync(FULL, b20));
+  const int start = S.vd0[S.ord[nvf]];
+  if (S.rptr[start] == (PIdx)T::NONE) return -1;
+  if (E > T::VMAX) return -1;
+  int ok = 1;
+  if (lane == 0) {
+    int cur = start;
+    for (int e = 0; e < E; e++) {
+      const int nxt = S.rptr[cur];
+      if (nxt == (int)T::NONE || (e < E - 1 && nxt == start)) {
+        ok = 0;
+        break;
+      }
+      S.ea[e] = (PIdx)cur;
+      S.eb[e] = (PIdx)nxt;
+      cur = nxt;
+    }
+    if (ok && cur != start) ok = 0;
+  }
+  ok = __shfl_sync(FULL, ok, 0);
+  __syncwarp();
+  return ok ? E : -1;
+}
+
+// --------------------------------------------------------------- integrals --
+// Scratch of the integral step: projections on the plane-pair lines of 5 vertices
+// and the 30 tets' values.
+struct TetScratch {
+  double ix[15], iy[15], iz[15];
+  double val[8][32];
+};
+
+// Integrals and face emission of a finished cell (convex_cell.rs:131-187,
+// voronoi_cell.rs:40-100) over a view V of the cell: V.normal(pl), V.d(pl),
+// V.proj(pl) (the generator projected on plane pl), V.right(pl), V.code(pl),
+// V.dual(q, i) and V.loc(q) for vertex position q in the reference's order.  Each
+// 5-vertex step projects on the 15 plane-pair lines, builds the 30 tets (one per
+// lane) and accumulates them in the reference's tet order: lanes 0-3 the cell
+// integrals, lane p (and p + 32k) the integrals of face p.
+template <class T, class View>
+__device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetScratch& Sc, int lane,
+                                              int self, D3 x, int nv, int np, double sr,
+                                              int* err_code) {
+  const int dim = J.dim;
+  double cacc = 0.0;  // lanes 0..3: volume, centroid x, y, z
+  double fa[T::PMAX / 32], fcx[T::PMAX / 32], fcy[T::PMAX / 32], fcz[T::PMAX / 32];
+  unsigned ftouched = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) fa[k] = 0.0, fcx[k] = 0.0, fcy[k] = 0.0, fcz[k] = 0.0;
+  for (int base = 0; base < nv; base += 5) {
+    const int nstep = min(5, nv - base);
+    // projections on the lines dual[i] & dual[i+1]: project_onto_intersection
+    // (geometry.rs:41-47) of plane dual[(i+1)%3] with dual[i]
+    bool ok = true;
+    if (lane < 3 * nstep) {
+      const int vl = lane / 3, i = lane - 3 * vl;
+      const int q = base + vl;
+      const int cur = V.dual(q, i);
+      const int nx = V.dual(q, i == 2 ? 0 : i + 1);
+      const D3 cn = V.normal(cur);
+      const D3 nn = V.normal(nx);
+      const D3 perp = cross(nn, cn);
+      D3 pr = {0.0, 0.0, 0.0};
+      ok = intersect3(nn, V.d(nx), cn, V.d(cur), perp, dot(x, perp), &pr);
+      Sc.ix[lane] = pr.x;
+      Sc.iy[lane] = pr.y;
+      Sc.iz[lane] = pr.z;
+    }
+    if (__any_sync(FULL, !ok)) {
+      *err_code = MV_ERR_DET;
+      return CELL_ERROR;
+    }
+    __syncwarp();
+    // DecompositionWithoutFaces: tet t of a vertex = (proj[t], proj[(t+5)%6], vertex)
+    // with proj[2i] on plane dual[i] and proj[2i+1] on the line (dual[i+1], dual[i])
+    if (lane < 6 * nstep) {
+      const int vl = lane / 6, t = lane - 6 * vl;
+      const int q = base + vl;
+      auto proj = [&](int qq) -> D3 {
+        const int i = qq >> 1;
+        if (qq & 1) return D3{Sc.ix[3 * vl + i], Sc.iy[3 * vl + i], Sc.iz[3 * vl + i]};
+        return V.proj(V.dual(q, i));
+      };
+      const D3 v0 = proj(t), v1 = proj(t == 0 ? 5 : t - 1);
+      const D3 vloc = V.loc(q);
+      const double vol = signed_volume_tet(v0, v1, vloc, x);
+      const D3 vc = scale(vol, add(add(add(v0, v1), vloc), x));
+      const double ar = signed_area_tri(v0, v1, vloc, x);
+      const D3 ac = scale(ar, add(add(v0, v1), vloc));
+      Sc.val[0][lane] = vol;
+      Sc.val[1][lane] = vc.x;
+      Sc.val[2][lane] = vc.y;
+      Sc.val[3][lane] = vc.z;
+      Sc.val[4][lane] = ar;
+      Sc.val[5][lane] = ac.x;
+      Sc.val[6][lane] = ac.y;
+      Sc.val[7][lane] = ac.z;
+    }
+    __syncwarp();
+    const int ntet = 6 * nstep;
+    if (lane < 4) {
+      for (int s = 0; s < ntet; s++) cacc = cacc + Sc.val[lane][s];
+    }
+#pragma unroll
+    for (int k = 0; k < T::PMAX / 32; k++) {
+      const int pl = lane + 32 * k;
+      if (pl < np) {
+        for (int vl = 0; vl < nstep; vl++) {
+          const int q = base + vl;
+          const int kk = V.dual(q, 0) == pl ? 0 : (V.dual(q, 1) == pl ? 1 : (V.dual(q, 2) == pl ? 2 : -1));
+          if (kk >= 0) {
+            const int s = 6 * vl + 2 * kk;
+            fa[k] = fa[k] + Sc.val[4][s];
+            fcx[k] = fcx[k] + Sc.val[5][s];
+            fcy[k] = fcy[k] + Sc.val[6][s];
+            fcz[k] = fcz[k] + Sc.val[7][s];
+            fa[k] = fa[k] + Sc.val[4][s + 1];
+            fcx[k] = fcx[k] + Sc.val[5][s + 1];
+            fcy[k] = fcy[k] + Sc.val[6][s + 1];
+            fcz[k] = fcz[k] + Sc.val[7][s + 1];
+            ftouched |= 1u << k;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // cell: VolumeCentroidIntegral::finalize (integrals.rs:97-105)
+  const double vol = __shfl_sync(FULL, cacc, 0);
+  const double nrm = vol > 0.0 ? 0.25 / vol : 0.0;
+  if (lane < 4 && lane > 0) J.centroid[3 * (int64_t)self + (lane - 1)] = cacc * nrm;
+  if (lane == 0) {
+    J.volume[self] = vol;
+    J.safety_radius[self] = sr;
+  }
+  // faces: ownership (voronoi_cell.rs:414-434) and emission in plane order
+  unsigned emit = 0;
+  int nf_mine = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) {
+    const int pl = lane + 32 * k;
+    bool e = false;
+    if (pl < np && ((ftouched >> k) & 1u)) {
+      const D3 nn = V.normal(pl);
+      e = vector_is_valid(dim, nn);
+      const int r = V.right(pl);
+      if (e && J.face_mode == MV_FACES_OWNED && r >= 0 && V.code(pl) == 13)
+        e = r > self || (J.mask != nullptr && J.mask[r] == 0);
+    }
+    emit |= (unsigned)e << k;
+    nf_mine += e;
+  }
+  const int nf = __reduce_add_sync(FULL, (unsigned)nf_mine);
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(J.face_counter, (unsigned long long)nf);
+  base = __shfl_sync(FULL, base, 0);
+  if ((long long)(base + nf) > J.face_cap) return CELL_FACE_OVERFLOW;  // host grows staging, reruns
+  if (lane == 0) {
+    J.face_count[self] = nf;
+    J.stage_off[self] = (int64_t)base;
+  }
+  int rank_base = 0;
+#pragma unroll
+  for (int k = 0; k < T::PMAX / 32; k++) {
+    const bool ek = (emit >> k) & 1u;
+    const unsigned bal = __ballot_sync(FULL, ek);
+    if (ek) {
+      const int pl = lane + 32 * k;
+      const int64_t f = (int64_t)base + rank_base + __popc(bal & lanemask_lt());
+      const double na = fa[k] > 0.0 ? 1.0 / (3.0 * fa[k]) : 0.0;
+      const D3 nn = V.normal(pl);
+      J.f_left[f] = self;
+      J.f_right[f] = V.right(pl);
+      J.f_area[f] = fa[k];
+      J.f_centroid[3 * f] = fcx[k] * na;
+      J.f_centroid[3 * f + 1] = fcy[k] * na;
+      J.f_centroid[3 * f + 2] = fcz[k] * na;
+      J.f_normal[3 * f] = nn.x;
+      J.f_normal[3 * f + 1] = nn.y;
+      J.f_normal[3 * f + 2] = nn.z;
+      J.f_code[f] = (uint8_t)V.code(pl);
+    }
+    rank_base += __popc(bal);
+  }
+  return CELL_DONE;
+}
+
+}  // namespace mv

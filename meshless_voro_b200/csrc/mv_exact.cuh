@@ -110,7 +110,7 @@ __device__ __forceinline__ S5 det2_small(int64_t a, int64_t b, const S5& c, cons
 }
 
 // Sign of the exact in-sphere determinant (geometry.rs:271-314).  Returns -1, 0, 1.
-__device__ __noinline__ int in_sphere_exact_sign(const int64_t a[3], const int64_t b[3],
+static __device__ __noinline__ int in_sphere_exact_sign(const int64_t a[3], const int64_t b[3],
                                                  const int64_t c[3], const int64_t d[3],
                                                  const int64_t v[3]) {
   // rows: x, y, z (small, 53-bit) and n (squared norm); columns b, c, d, v

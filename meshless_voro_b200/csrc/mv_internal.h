@@ -104,6 +104,23 @@ struct Job {
   unsigned long long* stats;  // [ST_COUNT]
 };
 
+// One chunk of the staged path: cells at processing positions [item0, item0 + nitems)
+// go through the shell, clip and integral kernels.
+struct StageJob {
+  int32_t item0;
+  int32_t nitems;
+  int32_t cstride;            // candidate-list entries per cell
+  uint32_t* cand;             // [nitems][cstride]: sorted position * 27 + shift code
+  int32_t* info;              // [nitems]: count | exhausted << 30, 0: inactive, -1: retry
+  int64_t* rec_off;           // [nitems]: word offset of the cell record, -1: none
+  double* rec;                // cell records (planes, vertices) for the integral kernel
+  int64_t rec_cap;            // record words available to the chunk
+  unsigned long long* rec_counter;
+  unsigned int* work;         // [3] work counters of the shell, clip and integral kernels
+  int32_t* retry_list;        // positions the fused kernel builds afterwards
+  unsigned int* retry_count;
+};
+
 // Normalised simulation volume, boundary planes (boundary.rs:14-47), uniform grid and
 // first shell radius of one tessellation (mv_api.cu).
 struct Setup {

@@ -1,0 +1,576 @@
+// mv_staged.cu -- the staged cell pipeline: shell, clip and integral kernels.
+//
+// The same per-cell construction as the fused kernel (mv_cells.cu), split in three
+// kernels over a chunk of cells so that each kernel keeps a small instruction
+// footprint and its own occupancy:
+//   1. shell_kernel gathers each cell's first neighbour shell (rtree_nn.rs:10-240
+//      up to the initial radius) and writes it sorted to a candidate list;
+//   2. clip_kernel runs ConvexCell::build (convex_cell.rs:316-356) over the list and
+//      writes the finished cell (planes, vertices in the reference's order) to a
+//      record;
+//   3. integrate_kernel evaluates the integrals and emits the faces
+//      (voronoi_cell.rs:40-100) from the record.
+// A cell whose list does not decide it (the stream continues past the first shell,
+// or the shell overflowed) goes to a retry list that the fused kernel builds from
+// scratch afterwards, so every cell still sees the reference's full neighbour stream.
+//
+// Filtered clipping keeps 32 consecutive candidates in the warp, one per lane, with
+// the division-free f32 test of the fused kernel.  A candidate is certified not to
+// remove vertex v when s32(c, v) > T(c); a certificate depends only on the pair, so
+// after a clip only the new vertices are tested against the waiting candidates and
+// the next candidate needing the f64 plane is one ballot away.
+#include <cfloat>
+#include <cstdint>
+
+#include "mv_cell_common.cuh"
+
+namespace mv {
+
+#ifndef MV_CLIP_MINB
+#define MV_CLIP_MINB 7
+#endif
+#ifndef MV_CLIP_WARPS
+#define MV_CLIP_WARPS 4
+#endif
+constexpr int SHELL_CMAX = 128;
+constexpr int SHELL_WARPS = 4;
+constexpr int CLIP_WARPS = MV_CLIP_WARPS;
+constexpr int INT_WARPS = 4;
+using TierClip = Tier<64, 64, SHELL_CMAX, 8, uint8_t, MV_CLIP_MINB>;
+
+// Words of a cell record with np planes and nv vertices: header (np, nv), safety
+// radius, plane normals / offsets / generator projections (7 np), vertex locations
+// (3 nv), right generators (int32) and plane codes + vertex duals (bytes).
+__host__ __device__ __forceinline__ int64_t rec_words(int np, int nv) {
+  return 2 + 7 * (int64_t)np + 3 * (int64_t)nv + (np + 1) / 2 + (np + 3 * nv + 7) / 8;
+}
+
+// ------------------------------------------------------------------- shell --
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) shell_kernel(const __grid_constant__ Job J,
+                                                           const __grid_constant__ StageJob SJ) {
+  __shared__ ShellBuf<SHELL_CMAX> bufs[WARPS];
+  __shared__ double ext_s[6];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  ShellBuf<SHELL_CMAX>& B = bufs[warp];
+  if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  __syncthreads();
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(SJ.work + 0, 1u);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= SJ.nitems) break;
+    const int spos = SJ.item0 + item;
+    const int self = __ldg(J.sid + spos);
+    if (J.mask != nullptr && J.mask[self] == 0) {
+      if (lane == 0) SJ.info[item] = 0;
+      continue;
+    }
+    const D3 x = load_gen(J, self);
+    bool all = false;
+    const int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, J.R0, 0.0, ext_s, &all);
+    if (cnt > SHELL_CMAX || cnt == 0) {
+      if (lane == 0) SJ.info[item] = -1;
+      continue;
+    }
+    sort_shell<SHELL_CMAX>(B, lane, cnt);
+    // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
+    // fused kernel reports the error otherwise
+    if ((int)(B.tie[0] / 27u) != self) {
+      if (lane == 0) SJ.info[item] = -1;
+      continue;
+    }
+    uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
+    for (int k = lane; k < cnt; k += 32) out[k] = (uint32_t)B.cpos[k] * 27u + B.tie[k] % 27u;
+    if (lane == 0) SJ.info[item] = cnt | (all ? (1 << 30) : 0);
+    __syncwarp();
+  }
+}
+
+// -------------------------------------------------------------------- clip --
+template <class T>
+struct ClipSmem {
+  using PIdx = typename T::PIdx;
+  // clipping planes (half_space.rs:9-19)
+  double pnx[T::PMAX], pny[T::PMAX], pnz[T::PMAX], pd[T::PMAX];
+  double ppx[T::PMAX], ppy[T::PMAX], ppz[T::PMAX];
+  int32_t pright[T::PMAX];  // original index of the right generator, -1: boundary
+  uint8_t pcode[T::PMAX];   // periodic shift code, 13: none
+  PIdx rptr[T::PMAX];       // ring successor (SimpleCycle::ptrs)
+  // vertices (convex_cell.rs:16-25) in fixed slots
+  double vx[T::VMAX], vy[T::VMAX], vz[T::VMAX], vr2[T::VMAX];
+  float4 f4[T::VMAX];  // f32 (v - x) for the filter
+  alignas(4) PIdx ord[T::VMAX];   // position -> slot; [0, nv) is the reference's order
+  PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
+  PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
+  unsigned long long cnt[ST_COUNT];
+};
+
+template <class T, int PREC>
+__device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int lane, int item,
+                         int self, int info, int* err_code, CellCount& cc) {
+  using PIdx = typename T::PIdx;
+  const D3 x = load_gen(J, self);
+  const int dim = J.dim;
+
+  // ---- ConvexCell::init (convex_cell.rs:294-312) ----
+  if (lane < 6) {
+    S.pnx[lane] = J.bn[lane][0], S.pny[lane] = J.bn[lane][1], S.pnz[lane] = J.bn[lane][2];
+    S.ppx[lane] = J.bp[lane][0], S.ppy[lane] = J.bp[lane][1], S.ppz[lane] = J.bp[lane][2];
+    S.pd[lane] = J.bd[lane];
+    S.pright[lane] = -1;
+    S.pcode[lane] = 13;
+  }
+  for (int i = lane; i < T::VMAX; i += 32) S.ord[i] = (PIdx)i;
+  __syncwarp();
+  {
+    int i0 = 0, i1 = 0, i2 = 0;
+    cuboid_duals(lane, &i0, &i1, &i2);
+    bool ok = true;
+    double r2 = 0.0;
+    if (lane < 8) ok = make_vertex<PIdx>(S, lane, i0, i1, i2, x, dim, &r2);
+    if (__any_sync(FULL, !ok)) {
+      *err_code = MV_ERR_DET;
+      return CELL_ERROR;
+    }
+  }
+  __syncwarp();
+  int nv = 8, np = 6;
+  double max_r2 = warp_max_nonneg(lane < 8 ? S.vr2[lane] : 0.0);
+  double sr = 2.0 * sqrt(max_r2);
+  float A32 = __double2float_ru(amax_of(max_r2, dim));
+  const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
+
+  // ---- ConvexCell::build over the candidate list (convex_cell.rs:316-356) ----
+  const int ncand = info & 0x3fffffff;
+  const bool exhausted = (info >> 30) & 1;
+  const uint32_t* list = SJ.cand + (int64_t)item * SJ.cstride;
+  bool finished = false;
+  for (int w0 = 1; w0 < ncand && !finished; w0 += 32) {
+    const int wn = min(32, ncand - w0);
+    const bool valid = lane < wn;
+    // candidate w0 + lane: location and offset as the reference computes them
+    // (convex_cell.rs:333-342), plus the f32 quantities of the filter
+    D3 g = {0.0, 0.0, 0.0};
+    double dist = 1.0;
+    int orig = 0, code = 13;
+    float ex = 0.f, ey = 0.f, ez = 0.f, h = 0.f, c0 = 0.f, c1 = 0.f;
+    bool bad = false, filt = false;
+    if (valid) {
+      const uint32_t pk = __ldg(list + w0 + lane);
+      const int cp = (int)(pk / 27u);
+      code = (int)(pk - (uint32_t)cp * 27u);
+      g = {__ldg(J.sx + cp), __ldg(J.sy + cp), __ldg(J.sz + cp)};
+      orig = __ldg(J.sid + cp);
+      if (code != 13) g = add(g, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+      const D3 dx = sub(x, g);
+      dist = sqrt(dot(dx, dx));
+      bad = !(dist > 0.0 && dist <= DBL_MAX);
+      if (PREC == MV_PRECISION_FILTERED) {
+        // s = e.a + |e|^2 / 2 is certified by T = c0 + c1 A with A >= |v - x| over the
+        // cell's vertices (the bound of setup_batch, split into its A-free and A parts)
+        filt = !bad && dist >= 1e-15 && dist <= 1e15 && x1 <= 1e15;
+        ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y), ez = __double2float_rn(dx.z);
+        h = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        const double e1 = fabs(dx.x) + fabs(dx.y) + fabs(dx.z);
+        const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
+        const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
+        const double t0 = dist * (errb_up + u64 * (11.0 * e1 + 14.0 * x1) + u32 * (4.03 * dist));
+        c0 = __double2float_ru(t0 * (1.0 + 1e-6) + 1e-40);
+        c1 = __double2float_ru(dist * (u64 * 11.0 + u32 * 5.02) * (1.0 + 1e-6));
+      }
+    }
+    // window-constant ballots: degenerate distance, f32 filter applicable
+    const unsigned mbad = __ballot_sync(FULL, valid && bad);
+    unsigned mfilt = 0u;
+    if (PREC == MV_PRECISION_FILTERED) mfilt = __ballot_sync(FULL, valid && filt && A32 <= 1e15f);
+    // beyond the safety radius (refreshed when a clip shrinks it)
+    unsigned mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
+    // the f32 offset of this lane's vertex (position lane) for the filter
+    float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
+    int k = 0;
+    for (;;) {
+      const unsigned evt = (mbad | mstop) & (k < 32 ? (FULL << k) : 0u);
+      const int limit = evt ? __ffs(evt) - 1 : wn;
+      const int k0 = k;
+      if (PREC == MV_PRECISION_FILTERED) {
+        // candidates certified to remove no vertex are consumed without their plane
+        while (k < limit && ((mfilt >> k) & 1u)) {
+          const float exk = __shfl_sync(FULL, ex, k), eyk = __shfl_sync(FULL, ey, k);
+          const float ezk = __shfl_sync(FULL, ez, k), hk = __shfl_sync(FULL, h, k);
+          const float Tk = __fmaf_ru(__shfl_sync(FULL, c1, k), A32, __shfl_sync(FULL, c0, k));
+          bool need = lane < nv && !(fmaf(ezk, fv.z, fmaf(eyk, fv.y, fmaf(exk, fv.x, hk))) > Tk);
+          if (nv > 32 && lane + 32 < nv) {
+            const float4 f = S.f4[S.ord[lane + 32]];
+            need = need || !(fmaf(ezk, f.z, fmaf(eyk, f.y, fmaf(exk, f.x, hk))) > Tk);
+          }
+          if (__any_sync(FULL, need)) break;
+          k++;
+        }
+      }
+      WCNT(cc, ST_NEIGHBOURS, k - k0);
+      if (k == limit) {
+        if (limit == wn) break;  // window consumed
+        if ((mbad >> k) & 1u) {
+          *err_code = MV_ERR_DEGENERATE;  // convex_cell.rs:342
+          return CELL_ERROR;
+        }
+        finished = true;  // safety radius reached (convex_cell.rs:343-345)
+        break;
+      }
+      const int e = k++;
+      WCNT(cc, ST_NEIGHBOURS, 1);
+      // ---- candidate e: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
+      const D3 ngb = shfl_d3(g, e);
+      const double de = __shfl_sync(FULL, dist, e);
+      const int orig_e = __shfl_sync(FULL, orig, e);
+      const int code_e = __shfl_sync(FULL, code, e);
+      bool filt_e = false;
+      float exe = 0.f, eye = 0.f, eze = 0.f, he = 0.f, Tk = 0.f;
+      if (PREC == MV_PRECISION_FILTERED) {
+        filt_e = (mfilt >> e) & 1u;
+        exe = __shfl_sync(FULL, ex, e), eye = __shfl_sync(FULL, ey, e);
+        eze = __shfl_sync(FULL, ez, e), he = __shfl_sync(FULL, h, e);
+        Tk = __fmaf_ru(__shfl_sync(FULL, c1, e), A32, __shfl_sync(FULL, c0, e));
+      }
+      const D3 dx = sub(x, ngb);
+      const D3 n = divs(dx, de);
+      const D3 p = scale(0.5, add(x, ngb));
+      const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
+      const double d = dot(n, p);
+      unsigned rm[T::NW];
+      int n_und = 0, n_ex = 0;
+#pragma unroll
+      for (int w = 0; w < T::NW; w++) {
+        const int q = lane + 32 * w;
+        bool removed = false;
+        if (q < nv) {
+          const int sl = S.ord[q];
+          bool decided = false;
+          if (PREC == MV_PRECISION_FILTERED && filt_e) {
+            const float4 f = S.f4[sl];
+            const float s = fmaf(eze, f.z, fmaf(eye, f.y, fmaf(exe, f.x, he)));
+            if (fabsf(s) > Tk) {
+              removed = s < 0.f;
+              decided = true;
+            }
+          }
+          if (!decided) {
+            n_und++;
+            const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
+            if (fabs(c) < errb) {
+              removed = exact_clip(J, S, sl, x, ngb) < 0;
+              n_ex++;
+            } else {
+              removed = c < 0.0;
+            }
+          }
+        }
+        rm[w] = __ballot_sync(FULL, removed);
+      }
+      n_und = (int)__reduce_add_sync(FULL, (unsigned)n_und);
+      n_ex = (int)__reduce_add_sync(FULL, (unsigned)n_ex);
+      if (PREC == MV_PRECISION_FILTERED) WCNT(cc, ST_F32_UNDECIDED, n_und);
+      WCNT(cc, ST_EXACT, n_ex);
+      int nrem = 0;
+#pragma unroll
+      for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
+      if (nrem == 0) continue;
+
+      // ---- a vertex was clipped: add the plane (convex_cell.rs:393-418) ----
+      if (np >= T::PMAX) return CELL_OVERFLOW;
+      const int p_idx = np;
+      if (lane == 0) {
+        S.pnx[p_idx] = n.x, S.pny[p_idx] = n.y, S.pnz[p_idx] = n.z;
+        S.ppx[p_idx] = p.x, S.ppy[p_idx] = p.y, S.ppz[p_idx] = p.z;
+        S.pd[p_idx] = d;
+        S.pright[p_idx] = orig_e;
+        S.pcode[p_idx] = (uint8_t)code_e;
+      }
+      np++;
+      WCNT(cc, ST_PLANES, 1);
+
+      // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
+      unsigned km[T::NW];
+      int totK = 0;
+#pragma unroll
+      for (int w = 0; w < T::NW; w++) {
+        km[w] = ~rm[w] & valid_bits(nv, w);
+        totK += __popc(km[w]);
+      }
+      const int nvf = totK;
+      {
+        int dest[T::NW];
+        PIdx held[T::NW];
+#pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int q = lane + 32 * w;
+          int dd = -1;
+          held[w] = 0;
+          if (q < nv) {
+            held[w] = S.ord[q];
+            if (!((rm[w] >> lane) & 1u)) {
+              dd = q < nvf ? q : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, q));
+            } else if (q <= nvf) {
+              const int t = rank_below<T::NW>(rm, q) + 1;
+              dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
+            } else {
+              dd = q - 1;
+            }
+          }
+          dest[w] = dd;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < T::NW; w++)
+          if (dest[w] >= 0) S.ord[dest[w]] = held[w];
+        __syncwarp();
+      }
+
+      // ring of the removed region (compute_boundary + SimpleCycle iteration)
+      int E = ring_parallel<T>(S, lane, nvf, nv);
+      if (E < 0) {
+        WCNT(cc, ST_SERIAL_RING, 1);
+        int e2 = 0;
+        if (lane == 0) e2 = ring_serial<T>(S, nvf, nv, np);
+        E = __shfl_sync(FULL, e2, 0);
+        __syncwarp();
+        if (E == -2) return CELL_OVERFLOW;
+        if (E < 0) {
+          *err_code = MV_ERR_RING;
+          return CELL_ERROR;
+        }
+      }
+      if (nvf + E > T::VMAX) return CELL_OVERFLOW;
+      bool ok = true;
+      double r2n = 0.0;
+      for (int ei = lane; ei < E; ei += 32)
+        ok &= make_vertex<PIdx>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
+      if (__any_sync(FULL, !ok)) {
+        *err_code = MV_ERR_DET;
+        return CELL_ERROR;
+      }
+      __syncwarp();
+      nv = nvf + E;
+      // update_safety_radius (convex_cell.rs:443-453)
+      double m = 0.0;
+      for (int q = lane; q < nv; q += 32) m = fmax(m, S.vr2[S.ord[q]]);
+      const double mr = warp_max_nonneg(m);
+      if (__double_as_longlong(mr) != __double_as_longlong(max_r2)) {
+        max_r2 = mr;
+        sr = 2.0 * sqrt(max_r2);
+        A32 = __double2float_ru(amax_of(max_r2, dim));
+      }
+      mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
+      if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
+    }
+  }
+  // the list ends: the shell was complete up to the initial radius (as the fused
+  // kernel's shell loop decides); otherwise the fused kernel continues the stream
+  if (!finished && !(exhausted || sr < J.R0 * (1.0 - 1e-12))) return CELL_RETRY;
+
+  // ---- the cell record for the integral kernel ----
+  const int64_t words = rec_words(np, nv);
+  unsigned long long off = 0;
+  if (lane == 0) off = atomicAdd(SJ.rec_counter, (unsigned long long)words);
+  off = __shfl_sync(FULL, off, 0);
+  if ((int64_t)off + words > SJ.rec_cap) return CELL_RETRY;
+  double* R = SJ.rec + off;
+  if (lane == 0) {
+    reinterpret_cast<int32_t*>(R)[0] = np;
+    reinterpret_cast<int32_t*>(R)[1] = nv;
+    R[1] = sr;
+  }
+  double* nx = R + 2;
+  double *ny = nx + np, *nz = ny + np, *dd = nz + np, *qx = dd + np, *qy = qx + np, *qz = qy + np;
+  double *vxo = qz + np, *vyo = vxo + nv, *vzo = vyo + nv;
+  int32_t* rt = reinterpret_cast<int32_t*>(vzo + nv);
+  uint8_t* pc = reinterpret_cast<uint8_t*>(vzo + nv + (np + 1) / 2);
+  uint8_t *d0 = pc + np, *d1 = d0 + nv, *d2 = d1 + nv;
+  for (int pl = lane; pl < np; pl += 32) {
+    const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
+    const D3 pr = plane_project(nn, {S.ppx[pl], S.ppy[pl], S.ppz[pl]}, x);
+    nx[pl] = nn.x, ny[pl] = nn.y, nz[pl] = nn.z, dd[pl] = S.pd[pl];
+    qx[pl] = pr.x, qy[pl] = pr.y, qz[pl] = pr.z;
+    rt[pl] = S.pright[pl];
+    pc[pl] = S.pcode[pl];
+  }
+  for (int q = lane; q < nv; q += 32) {
+    const int sl = S.ord[q];
+    vxo[q] = S.vx[sl], vyo[q] = S.vy[sl], vzo[q] = S.vz[sl];
+    d0[q] = (uint8_t)S.vd0[sl], d1[q] = (uint8_t)S.vd1[sl], d2[q] = (uint8_t)S.vd2[sl];
+  }
+  if (lane == 0) SJ.rec_off[item] = (int64_t)off;
+  __syncwarp();
+  return CELL_DONE;
+}
+
+template <class T, int PREC, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_constant__ Job J,
+                                                                  const __grid_constant__ StageJob SJ) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  ClipSmem<T>& S = reinterpret_cast<ClipSmem<T>*>(smem_raw)[warp];
+  if (lane < ST_COUNT) S.cnt[lane] = 0ull;
+  __syncwarp();
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(SJ.work + 1, 1u);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= SJ.nitems) break;
+    const int spos = SJ.item0 + item;
+    const int self = __ldg(J.sid + spos);
+    if (J.mask != nullptr && J.mask[self] == 0) {
+      // VoronoiCell::default() (voronoi.rs:303-305)
+      if (lane < 3) J.centroid[3 * (int64_t)self + lane] = 0.0;
+      if (lane == 0) {
+        J.volume[self] = 0.0;
+        J.safety_radius[self] = 0.0;
+        J.face_count[self] = 0;
+        J.stage_off[self] = 0;
+        SJ.rec_off[item] = -1;
+      }
+      continue;
+    }
+    const int info = SJ.info[item];
+    int res = CELL_RETRY;
+    int err = 0;
+    CellCount cc;
+#pragma unroll
+    for (int i = 0; i < ST_COUNT; i++) cc.c[i] = 0u;
+    if (info > 0) res = clip_cell<T, PREC>(J, SJ, S, lane, item, self, info, &err, cc);
+    __syncwarp();
+    if (lane == 0) {
+      if (res == CELL_DONE) {
+#pragma unroll
+        for (int i = 0; i < ST_COUNT; i++) S.cnt[i] += cc.c[i];
+      } else {
+        SJ.rec_off[item] = -1;
+        if (res == CELL_ERROR) {
+          atomicCAS(J.status + STATUS_CODE, 0, err);
+          atomicMin(J.status + STATUS_CELL, self);
+        } else {
+          const unsigned k = atomicAdd(SJ.retry_count, 1u);
+          SJ.retry_list[k] = spos;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J.stats + lane, S.cnt[lane]);
+}
+
+// --------------------------------------------------------------- integrals --
+// A cell record as the integral step reads it.
+struct RecordView {
+  const double *nx, *ny, *nz, *dd, *qx, *qy, *qz, *vx, *vy, *vz;
+  const int32_t* rt;
+  const uint8_t *pc, *d0, *d1, *d2;
+  __device__ D3 normal(int pl) const { return {__ldg(nx + pl), __ldg(ny + pl), __ldg(nz + pl)}; }
+  __device__ double d(int pl) const { return __ldg(dd + pl); }
+  __device__ D3 proj(int pl) const { return {__ldg(qx + pl), __ldg(qy + pl), __ldg(qz + pl)}; }
+  __device__ int right(int pl) const { return __ldg(rt + pl); }
+  __device__ int code(int pl) const { return __ldg(pc + pl); }
+  __device__ int dual(int q, int i) const {
+    return i == 0 ? __ldg(d0 + q) : (i == 1 ? __ldg(d1 + q) : __ldg(d2 + q));
+  }
+  __device__ D3 loc(int q) const { return {__ldg(vx + q), __ldg(vy + q), __ldg(vz + q)}; }
+};
+
+template <class T, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) integrate_kernel(const __grid_constant__ Job J,
+                                                               const __grid_constant__ StageJob SJ) {
+  __shared__ TetScratch scratch[WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned done = 0;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(SJ.work + 2, 1u);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= SJ.nitems) break;
+    const int64_t off = SJ.rec_off[item];
+    if (off < 0) continue;
+    const int spos = SJ.item0 + item;
+    const int self = __ldg(J.sid + spos);
+    const D3 x = load_gen(J, self);
+    const double* R = SJ.rec + off;
+    const int np = __ldg(reinterpret_cast<const int32_t*>(R));
+    const int nv = __ldg(reinterpret_cast<const int32_t*>(R) + 1);
+    const double sr = __ldg(R + 1);
+    RecordView V;
+    V.nx = R + 2, V.ny = V.nx + np, V.nz = V.ny + np, V.dd = V.nz + np;
+    V.qx = V.dd + np, V.qy = V.qx + np, V.qz = V.qy + np;
+    V.vx = V.qz + np, V.vy = V.vx + nv, V.vz = V.vy + nv;
+    V.rt = reinterpret_cast<const int32_t*>(V.vz + nv);
+    V.pc = reinterpret_cast<const uint8_t*>(V.vz + nv + (np + 1) / 2);
+    V.d0 = V.pc + np, V.d1 = V.d0 + nv, V.d2 = V.d1 + nv;
+    int err = 0;
+    const int res = integrate_view<T>(J, V, scratch[warp], lane, self, x, nv, np, sr, &err);
+    if (res == CELL_DONE) {
+      done++;
+    } else if (lane == 0) {
+      if (res == CELL_FACE_OVERFLOW) {
+        atomicExch(J.status + STATUS_FACE_OVERFLOW, 1);
+      } else {
+        atomicCAS(J.status + STATUS_CODE, 0, err);
+        atomicMin(J.status + STATUS_CELL, self);
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && done) atomicAdd(J.stats + ST_CELLS, (unsigned long long)done);
+}
+
+// ---------------------------------------------------------------- launchers --
+template <class K>
+static int occupancy(K k, int threads, size_t smem) {
+  int nb = 0;
+  if (smem > 0 &&
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
+  return nb;
+}
+
+constexpr size_t CLIP_SMEM = sizeof(ClipSmem<TierClip>) * CLIP_WARPS;
+
+int stage_blocks_per_sm(int kernel, int precision) {
+  if (kernel == 0) return occupancy(shell_kernel<SHELL_WARPS>, 32 * SHELL_WARPS, 0);
+  if (kernel == 1)
+    return precision == MV_PRECISION_FILTERED
+               ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>, 32 * CLIP_WARPS,
+                           CLIP_SMEM)
+               : occupancy(clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS>, 32 * CLIP_WARPS,
+                           CLIP_SMEM);
+  return occupancy(integrate_kernel<TierClip, INT_WARPS>, 32 * INT_WARPS, 0);
+}
+
+int stage_list_stride() { return SHELL_CMAX; }
+
+int64_t stage_record_words(int np, int nv) { return rec_words(np, nv); }
+
+cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st) {
+  if (blocks < 1) blocks = 1;
+  if (kernel == 0) {
+    shell_kernel<SHELL_WARPS><<<blocks, 32 * SHELL_WARPS, 0, st>>>(J, SJ);
+  } else if (kernel == 1) {
+    if (J.precision == MV_PRECISION_FILTERED) {
+      auto k = clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>;
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
+      if (e != cudaSuccess) return e;
+      k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ);
+    } else {
+      auto k = clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS>;
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
+      if (e != cudaSuccess) return e;
+      k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ);
+    }
+  } else {
+    integrate_kernel<TierClip, INT_WARPS><<<blocks, 32 * INT_WARPS, 0, st>>>(J, SJ);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace mv

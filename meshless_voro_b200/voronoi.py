@@ -56,8 +56,12 @@ def shift_from_code(code: int, width) -> Optional[np.ndarray]:
     return out
 
 
+PIPELINE = {"auto": N.MV_PIPELINE_AUTO, "staged": N.MV_PIPELINE_STAGED, "fused": N.MV_PIPELINE_FUSED}
+
+
 def make_options(precision="filtered", face_mode=N.MV_FACES_OWNED, stream=None,
-                 points_per_grid_cell=0.0, initial_radius=0.0) -> N.Options:
+                 points_per_grid_cell=0.0, initial_radius=0.0, pipeline="auto",
+                 chunk_cells=0) -> N.Options:
     o = N.Options()
     N.lib().mv_options_default(C.byref(o))
     o.precision = PRECISION[precision] if isinstance(precision, str) else int(precision)
@@ -65,6 +69,8 @@ def make_options(precision="filtered", face_mode=N.MV_FACES_OWNED, stream=None,
     o.points_per_grid_cell = float(points_per_grid_cell)
     o.initial_radius = float(initial_radius)
     o.stream = stream
+    o.pipeline = PIPELINE[pipeline] if isinstance(pipeline, str) else int(pipeline)
+    o.chunk_cells = int(chunk_cells)
     return o
 
 

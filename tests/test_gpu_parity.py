@@ -107,20 +107,26 @@ def compare(gpu, orc, faces_all=False):
             and np.array_equal(gpu.face_centroid, orc.face_centroid))
 
 
+# the staged pipeline runs in small chunks so that every case spans several of them
+PIPELINES = {"fused": dict(pipeline="fused"), "staged": dict(pipeline="staged", chunk_cells=997)}
+
+
+@pytest.mark.parametrize("pipeline", ["fused", "staged"])
 @pytest.mark.parametrize("precision", ["fp64", "filtered"])
 @pytest.mark.parametrize("name", CASES)
-def test_parity_full_build(gpu_ctx, oracle, name, precision):
+def test_parity_full_build(gpu_ctx, oracle, name, precision, pipeline):
     c = _case(name)
     orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"], periodic=c["periodic"])
     gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], c["dim"],
-                               c["periodic"], precision=precision)
+                               c["periodic"], precision=precision, **PIPELINES[pipeline])
     bit_identical = compare(gpu, orc)
     assert bit_identical, "expected bit-identical integrals"
 
 
+@pytest.mark.parametrize("pipeline", ["fused", "staged"])
 @pytest.mark.parametrize("precision", ["fp64", "filtered"])
 @pytest.mark.parametrize("name", ["grid15_w2", "poisson20k_periodic", "plane25_periodic_2d"])
-def test_parity_partial(gpu_ctx, oracle, name, precision):
+def test_parity_partial(gpu_ctx, oracle, name, precision, pipeline):
     c = _case(name)
     n = len(c["generators"])
     rng = np.random.default_rng(7)
@@ -128,20 +134,40 @@ def test_parity_partial(gpu_ctx, oracle, name, precision):
         orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"],
                            periodic=c["periodic"], mask=mask)
         gpu = gpu_ctx.build_arrays(c["generators"], mask, c["anchor"], c["width"], c["dim"],
-                                   c["periodic"], precision=precision)
+                                   c["periodic"], precision=precision, **PIPELINES[pipeline])
         assert compare(gpu, orc)
         assert np.all(gpu.cell_volume[~mask] == 0.0)
 
 
+@pytest.mark.parametrize("pipeline", ["fused", "staged"])
 @pytest.mark.parametrize("name", ["grid15_w2", "poisson20k_periodic", "plane25_periodic_2d"])
-def test_parity_all_faces_integrator(gpu_ctx, oracle, name):
+def test_parity_all_faces_integrator(gpu_ctx, oracle, name, pipeline):
     """compute_face_integrals (non-symmetric): every face of every cell."""
     c = _case(name)
     orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=c["dim"],
                        periodic=c["periodic"], flags=oracle.FACES_ALL | oracle.NO_CSR)
     gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], c["dim"],
-                               c["periodic"], face_mode=MV_FACES_ALL)
+                               c["periodic"], face_mode=MV_FACES_ALL, **PIPELINES[pipeline])
     assert compare(gpu, orc, faces_all=True)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "filtered"])
+def test_staged_retry_and_stats(gpu_ctx, oracle, precision):
+    """A small initial radius sends many cells to the fused retry pass; the result and
+    the per-cell counters must not depend on which kernel built a cell."""
+    c = _case("poisson20k_periodic")
+    orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=3, periodic=True)
+    stats = {}
+    for pipe, kw in (("fused", dict(pipeline="fused")),
+                     ("staged", dict(pipeline="staged", chunk_cells=4096, initial_radius=1.6))):
+        gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], 3, True,
+                                   precision=precision, **kw)
+        assert compare(gpu, orc)
+        stats[pipe] = gpu_ctx.last_stats()
+    assert stats["staged"]["staged_retries"] > 0
+    assert stats["fused"]["staged_retries"] == 0
+    for k in ("cells_built", "neighbours_clipped", "planes_added", "exact_tests", "serial_rings"):
+        assert stats["staged"][k] == stats["fused"][k], k
 
 
 def test_reference_api_kats(gpu_ctx):
