@@ -120,7 +120,7 @@ int make_setup(int64_t n, const double* anchor, const double* width, int dim, in
     s->geps[i] = 1e-9 * s->gh[i] + 1e-13 * (std::fabs(aa[i]) + ww[i]);
   }
   const double spacing = std::pow(vol / nn, 1.0 / dim);
-  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.6 : (dim == 2 ? 2.4 : 2.2));
+  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.8 : (dim == 2 ? 2.4 : 2.2));
   s->R0 = r0 * spacing;
   return MV_OK;
 }

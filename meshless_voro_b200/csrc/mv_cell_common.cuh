@@ -197,6 +197,15 @@ __device__ __forceinline__ double amax_of(double max_r2, int dim) {
   return sqrt((max_r2 + 0.26 * (3 - dim)) * (1.0 + 1e-9)) * (1.0 + 1e-9);
 }
 
+// The same bound in f32, rounded up, from the safety radius sr = 2 sqrt(max_r2):
+// sqrt(max_r2) <= sr / 2 (1 + 2^-52), |v - x| exceeds the rounded sqrt(max_r2) by a
+// few ulps at most, and sqrt(a + b) <= sqrt(a) + sqrt(b) covers the extruded
+// dimensions (sqrt(0.26) < 0.51, sqrt(0.52) < 0.7212).
+__device__ __forceinline__ float amax32_of_sr(double sr, int dim) {
+  const float h = __fmul_ru(__double2float_ru(sr), 0.50000006f);
+  return dim == 3 ? h : __fadd_ru(h, dim == 2 ? 0.51f : 0.7212f);
+}
+
 enum CellResult {
   CELL_DONE = 0,
   CELL_OVERFLOW = 1,

@@ -138,7 +138,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   int nv = 8, np = 6;
   double max_r2 = warp_max_nonneg(lane < 8 ? S.vr2[lane] : 0.0);
   double sr = 2.0 * sqrt(max_r2);
-  float A32 = __double2float_ru(amax_of(max_r2, dim));
+  float A32 = amax32_of_sr(sr, dim);
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
 
   // ---- ConvexCell::build over the candidate list (convex_cell.rs:316-356) ----
@@ -360,7 +360,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       if (__double_as_longlong(mr) != __double_as_longlong(max_r2)) {
         max_r2 = mr;
         sr = 2.0 * sqrt(max_r2);
-        A32 = __double2float_ru(amax_of(max_r2, dim));
+        A32 = amax32_of_sr(sr, dim);
       }
       mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
       if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
