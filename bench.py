@@ -8,6 +8,10 @@ uniform generators in the periodic unit box (seeded, synthetic).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision filtered|fp64]
                   [--workload poisson_256|lattice_64|jitter_32] [--impl ours|reference]
+                  [--pipeline auto|staged|fused]
+
+The default pipeline runs the staged shell / clip / integral kernels; the plain FP64
+comparison is the fused one-kernel-per-cell FP64 build of the same workload.
 
 With N > 1 (torchrun, one process per GPU) every rank tessellates its own
 independently seeded generator set (weak scaling, no collective on the data path);
@@ -30,12 +34,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "3D Voronoi cells/s on 1 B200: FP32-filtered batched vs plain FP64, exact topology"
 HBM_PEAK_FALLBACK = 6650.0
-# DRAM bytes (read + write) per cell of the cell kernel, from one ncu capture of the
-# 64^3 periodic Poisson case (profiles/cells_kernel_poisson64.md); traffic grows in
+# DRAM bytes (read + write) per cell of the clip kernel, from one ncu capture of the
+# 64^3 periodic Poisson case (profiles/clip_kernel_poisson64.md); traffic grows in
 # proportion to the cells, so a launch's traffic is this figure times its cells.
-CELLS_KERNEL_DRAM_BYTES_PER_CELL = 647.8
+CLIP_KERNEL_DRAM_BYTES_PER_CELL = 2770.6
 # algorithmic bytes (generator read + cell outputs + owned faces + CSR entries)
 BYTES_GEN, BYTES_CELL, BYTES_FACE, BYTES_CONN = 24, 40, 68, 4
+# cells per chunk of the staged pipeline (library default)
+CHUNK_CELLS = 1 << 20
 
 
 def rank_seed(rank: int, base: int = 3) -> int:
@@ -206,6 +212,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson_256")
     ap.add_argument("--precision", default="filtered", choices=["filtered", "fp64"])
+    ap.add_argument("--pipeline", default="auto", choices=["auto", "staged", "fused"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 side run")
@@ -238,45 +245,55 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
 
-    def step(precision):
+    def step(precision, pipeline):
         return ctx.build_device(g_dev.data_ptr(), 0, n, w["anchor"], w["width"],
                                 w["dimensionality"], w["periodic"], precision=precision,
-                                stream=sp)
+                                stream=sp, pipeline=pipeline)
 
-    def timed(precision, steps):
+    def timed(precision, steps, pipeline=args.pipeline):
         for _ in range(args.warmup):
-            step(precision)
+            step(precision, pipeline)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        cells_ms, stats, out = [], None, None
+        per_step, stats, out = [], None, None
         e0.record(stream)
         for _ in range(steps):
-            out = step(precision)
+            out = step(precision, pipeline)
             stats = ctx.last_stats()
-            cells_ms.append(stats["ms_cells"])
+            per_step.append(stats)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, dev)
         if world > 1:
             dist.barrier()
-        return ms, float(np.mean(cells_ms)), stats, out
+        # device times of the cell phase and its kernels (library CUDA events on `stream`)
+        kms = {k: float(np.mean([st[k] for st in per_step]))
+               for k in ("ms_cells", "ms_shell", "ms_clip", "ms_integrate", "ms_retry")}
+        return ms, kms, stats, out
 
     with ClockSampler(local) as clk:
-        ms, cells_ms, stats, out = timed(args.precision, args.steps)
+        ms, kms, stats, out = timed(args.precision, args.steps)
     clocks = clk.summary()
     F, Cn = int(out.n_faces), int(out.n_connections)
     value = aggregate_cells_per_s(world, n, ms)
+    cells_ms = kms["ms_cells"]
 
-    # plain FP64 kernel side by side (same workload, same step)
+    # side by side: the other precision on the same pipeline, and the plain FP64 build
+    # (the fused one-kernel-per-cell kernel, f64 predicates throughout)
     other = None
     if not args.no_compare:
+        other = []
         o_prec = "fp64" if args.precision == "filtered" else "filtered"
-        o_ms, o_cells_ms, o_stats, _ = timed(o_prec, max(2, args.steps // 2))
-        other = {"precision": o_prec, "value": aggregate_cells_per_s(world, n, o_ms),
-                 "ms_per_step": o_ms, "cells_kernel_ms": o_cells_ms,
-                 "f32_undecided": o_stats["f32_undecided"], "exact_tests": o_stats["exact_tests"]}
+        for prec, pipe, label in ((o_prec, args.pipeline, f"{o_prec}, same pipeline"),
+                                  ("fp64", "fused", "plain FP64 per-cell kernel (fused)")):
+            o_ms, o_kms, o_stats, _ = timed(prec, max(2, args.steps // 2), pipe)
+            other.append({"label": label, "precision": prec, "pipeline": pipe,
+                          "value": aggregate_cells_per_s(world, n, o_ms), "ms_per_step": o_ms,
+                          "cells_ms": o_kms["ms_cells"],
+                          "f32_undecided": o_stats["f32_undecided"],
+                          "exact_tests": o_stats["exact_tests"]})
 
     # end to end through the C ABI with host buffers (pinned input, results to pinned host)
     e2e = None
@@ -312,13 +329,31 @@ def main():
                "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
 
     peak, peak_kind = measured_peaks()
+    # algorithmic bytes of the whole path for this workload (generator read, cell and
+    # face outputs, CSR), counted from the run's own output
     alg_bytes = BYTES_GEN * n + BYTES_CELL * n + BYTES_FACE * F + BYTES_CONN * Cn
-    achieved = alg_bytes / (cells_ms * 1e-3) / 1e9
-    traffic = CELLS_KERNEL_DRAM_BYTES_PER_CELL * n if args.workload.startswith("poisson") else None
+    staged = kms["ms_clip"] > 0.0
+    if staged:
+        # dominant kernel: the clip kernel; one launch per chunk of cells
+        chunk = min(n, CHUNK_CELLS)
+        launches = -(-n // chunk)
+        per_launch_ms = kms["ms_clip"] / launches
+        per_launch_bytes = alg_bytes * chunk / n
+        traffic = (CLIP_KERNEL_DRAM_BYTES_PER_CELL * chunk
+                   if args.workload.startswith("poisson") else None)
+        kernel = "mv::clip_kernel (staged pipeline)"
+    else:
+        per_launch_ms, per_launch_bytes, traffic = cells_ms, alg_bytes, None
+        kernel = "mv::cells_kernel (fused pipeline)"
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "mv::cells_kernel", "alg_bytes_per_launch": alg_bytes,
-                "kernel_ms": cells_ms}
+                "kernel": kernel, "alg_bytes_per_launch": per_launch_bytes,
+                "kernel_ms_per_launch": per_launch_ms,
+                "phase": {"kernels": "cell construction (all cell kernels)",
+                          "achieved": alg_bytes / (cells_ms * 1e-3) / 1e9, "ms": cells_ms},
+                "kernels_ms": {"shell": kms["ms_shell"], "clip": kms["ms_clip"],
+                               "integrate": kms["ms_integrate"], "retry": kms["ms_retry"]}}
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -330,7 +365,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
                 "config": {"workload": w["name"], "n_generators": n, "periodic": w["periodic"],
-                           "precision": args.precision, "parallelism": f"weak{world}",
+                           "precision": args.precision, "pipeline": args.pipeline,
+                           "parallelism": f"weak{world}",
                            "cache": "inputs larger than L2 (403 MB generators)"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
                 "gpu_launches": int(stats["kernel_launches"]) * args.steps,
@@ -344,7 +380,8 @@ def main():
                            "exact_tests": stats["exact_tests"],
                            "extra_shells": stats["extra_shells"],
                            "overflow_cells": stats["overflow_cells"],
-                           "serial_rings": stats["serial_rings"]},
+                           "serial_rings": stats["serial_rings"],
+                           "staged_retries": stats["staged_retries"]},
                 "side_by_side": other}
         print(json.dumps(line), flush=True)
     ctx.close()

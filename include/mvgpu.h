@@ -85,6 +85,10 @@ typedef struct mv_build_stats {
   double ms_grid;                /* device time: generator prep + uniform grid       */
   double ms_cells;               /* device time: cell construction kernels           */
   double ms_finalize;            /* device time: face ordering + cell->face CSR      */
+  double ms_shell;               /* staged pipeline, within ms_cells: shell kernels  */
+  double ms_clip;                /*   clip kernels                                   */
+  double ms_integrate;           /*   integral kernels                               */
+  double ms_retry;               /*   fused kernel on the retried cells              */
 } mv_build_stats;
 
 /* Device-resident result of a build.  Pointers are owned by the context and stay

@@ -53,7 +53,8 @@ class BuildStats(C.Structure):
         "cells_built", "neighbours_clipped", "planes_added", "f32_undecided", "exact_tests",
         "extra_shells", "overflow_cells", "serial_rings", "staged_retries", "device_bytes",
         "kernel_launches")] + [
-        (name, C.c_double) for name in ("ms_grid", "ms_cells", "ms_finalize")]
+        (name, C.c_double) for name in ("ms_grid", "ms_cells", "ms_finalize", "ms_shell",
+                                         "ms_clip", "ms_integrate", "ms_retry")]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

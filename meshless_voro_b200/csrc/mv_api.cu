@@ -160,6 +160,7 @@ struct mv_context {
   int bps_fast[2] = {0, 0};
   int bps_large[2] = {0, 0};
   int bps_stage[3][2] = {};  // shell, clip, integral kernels by precision
+  std::vector<cudaEvent_t> stage_ev;  // 4 per chunk: before shell, clip, integral, after
   double rec_words_hint = 0.0;  // record words per cell the last staged build needed
   Workspace ws;
   size_t dev_bytes = 0;
@@ -240,7 +241,7 @@ int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224
 // Cells the first shell does not decide are appended to the retry list; *n_retry
 // receives their number.
 int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& o, int64_t n,
-               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry) {
+               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry, double ms_stage[3]) {
   Workspace& W = ctx->ws;
   const int64_t chunk = std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
   const int64_t nchunks = (n + chunk - 1) / chunk;
@@ -259,6 +260,11 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
   if (e) return MV_ERR_OOM;
   unsigned long long* ctr = P<unsigned long long>(W.stage_ctr);
   MV_CUDA(cudaMemsetAsync(ctr, 0, 8 * ctr_words, st));
+  while (ctx->stage_ev.size() < 4 * (size_t)nchunks) {
+    cudaEvent_t ev;
+    MV_CUDA(cudaEventCreate(&ev));
+    ctx->stage_ev.push_back(ev);
+  }
   StageJob SJ;
   std::memset(&SJ, 0, sizeof(SJ));
   SJ.cstride = stride;
@@ -279,14 +285,24 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
       const int wpb = 4;  // every stage kernel runs 4 warps per block
       int64_t blocks = (int64_t)ctx->sm_count * std::max(1, ctx->bps_stage[k][pi]);
       blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
+      MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + k], st));
       MV_CUDA(launch_stage(k, J, SJ, (int)std::max<int64_t>(1, blocks), st));
       (*launches)++;
     }
+    MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
   }
   std::vector<unsigned long long> h(ctr_words);
   MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * ctr_words, cudaMemcpyDeviceToHost, st));
   MV_CUDA(cudaStreamSynchronize(st));
   *n_retry = (int64_t)(h[0] & 0xffffffffull);
+  for (int k = 0; k < 3; k++) ms_stage[k] = 0.0;
+  for (int64_t c = 0; c < nchunks; c++) {
+    for (int k = 0; k < 3; k++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ctx->stage_ev[4 * c + k], ctx->stage_ev[4 * c + k + 1]);
+      ms_stage[k] += t;
+    }
+  }
   // size the record buffer of the next build by what this one asked for
   double need = 0.0;
   for (int64_t c = 0; c < nchunks; c++) {
@@ -444,9 +460,10 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     const bool staged = use_staged(o, n);
     bool retry_ran = false;
     int64_t n_retry = 0;
+    double ms_stage[3] = {0.0, 0.0, 0.0};
     MV_CUDA(cudaEventRecord(ctx->ev[1], st));
     if (n > 0 && staged) {
-      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry);
+      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry, ms_stage);
       if (rc2) return rc2;
       MV_CUDA(cudaEventRecord(ctx->ev[2], st));
       if (n_retry > 0) {
@@ -472,6 +489,9 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     ctx->retry_ran = retry_ran;
     stats.staged_retries = n_retry;
+    stats.ms_shell = ms_stage[0];
+    stats.ms_clip = ms_stage[1];
+    stats.ms_integrate = ms_stage[2];
     bool large_ran = false;
     DevCounters hc;
     MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
@@ -572,6 +592,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     cudaEventElapsedTime(&t56, ctx->ev[5], ctx->ev[6]);
     stats.ms_grid = t01;
     stats.ms_cells = t12 + t34 + t78;
+    stats.ms_retry = t78;
     stats.ms_finalize = t56;
   }
   ctx->last = stats;
@@ -840,6 +861,7 @@ void mv_context_destroy(mv_context* ctx) {
   for (size_t i = 0; i < nb; i++)
     if (bufs[i].p) cudaFree(bufs[i].p);
   if (ctx->host) cudaFreeHost(ctx->host);
+  for (cudaEvent_t ev : ctx->stage_ev) cudaEventDestroy(ev);
   for (int i = 0; i < 10; i++)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   cudaStreamDestroy(ctx->stream);
