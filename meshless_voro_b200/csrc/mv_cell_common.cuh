@@ -550,6 +550,78 @@ __device__ __forceinline__ int ring_parallel(SM& S, int lane, int nvf, int nv) {
   return ok ? E : -1;
 }
 
+// Parallel ring with ranked edges: as ring_parallel, but each boundary edge goes to
+// its own lane, and its position in the SimpleCycle iteration order (starting at the
+// first removed vertex's dual[0]) comes from pointer jumping over warp shuffles
+// instead of a walk.  Lane e < E receives edge (*eu -> *ew) at ring position *erank.
+// Returns E, or -1 when the serial replay must decide (the start node is interior,
+// the edges do not form one cycle through it, or more than 32 edges).
+template <class T, class SM>
+__device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int* eu, int* ew,
+                                           int* erank) {
+  using PIdx = typename T::PIdx;
+  const int r = nv - nvf;
+  if (r > 32) return -1;
+  int t0 = 0, t1 = 0, t2 = 0;
+  if (lane < r) {
+    const int sl = S.ord[nvf + lane];
+    t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
+    S.rptr[t0] = (PIdx)T::NONE;
+    S.rptr[t1] = (PIdx)T::NONE;
+    S.rptr[t2] = (PIdx)T::NONE;
+  }
+  const int start = S.vd0[S.ord[nvf]];
+  __syncwarp();
+  // an edge u->w of a removed triangle is on the boundary iff no other removed
+  // triangle holds w->u
+  bool b01 = lane < r, b12 = lane < r, b20 = lane < r;
+  for (int k = 0; k < r; k++) {
+    const int a = __shfl_sync(FULL, t0, k), b = __shfl_sync(FULL, t1, k),
+              c = __shfl_sync(FULL, t2, k);
+    if (k == lane) continue;
+    b01 = b01 && !((a == t1 && b == t0) || (b == t1 && c == t0) || (c == t1 && a == t0));
+    b12 = b12 && !((a == t2 && b == t1) || (b == t2 && c == t1) || (c == t2 && a == t1));
+    b20 = b20 && !((a == t0 && b == t2) || (b == t0 && c == t2) || (c == t0 && a == t2));
+  }
+  const unsigned m01 = __ballot_sync(FULL, b01), m12 = __ballot_sync(FULL, b12),
+                 m20 = __ballot_sync(FULL, b20);
+  const int n01 = __popc(m01), n12 = __popc(m12);
+  const int E = n01 + n12 + __popc(m20);
+  if (E > 32) return -1;
+  // compact the edges: edge index by ballot rank; rptr maps a node to the edge leaving it
+  const unsigned lt = lanemask_lt();
+  const int p01 = __popc(m01 & lt), p12 = n01 + __popc(m12 & lt), p20 = n01 + n12 + __popc(m20 & lt);
+  if (b01) S.ea[p01] = (PIdx)t0, S.eb[p01] = (PIdx)t1, S.rptr[t0] = (PIdx)p01;
+  if (b12) S.ea[p12] = (PIdx)t1, S.eb[p12] = (PIdx)t2, S.rptr[t1] = (PIdx)p12;
+  if (b20) S.ea[p20] = (PIdx)t2, S.eb[p20] = (PIdx)t0, S.rptr[t2] = (PIdx)p20;
+  __syncwarp();
+  int u = 0, w = 0, nx = lane, d = 0;
+  bool broken = false;
+  if (lane < E) {
+    u = S.ea[lane], w = S.eb[lane];
+    nx = S.rptr[w];
+    d = 1;
+    // two boundary edges leave u, or none leaves w
+    broken = S.rptr[u] != (PIdx)lane || nx == (int)T::NONE;
+  }
+  const int se = S.rptr[start];
+  __syncwarp();
+  if (__any_sync(FULL, broken) || se == (int)T::NONE) return -1;
+  // distance from each edge to the start edge along the cycle
+  if (lane == se) nx = lane, d = 0;
+  for (int span = 1; span < E; span <<= 1) {
+    const int dn = __shfl_sync(FULL, d, nx);
+    const int nn = __shfl_sync(FULL, nx, nx);
+    d += dn;
+    nx = nn;
+  }
+  if (__any_sync(FULL, lane < E && nx != se)) return -1;  // not one cycle through the start
+  *eu = u;
+  *ew = w;
+  *erank = d == 0 ? 0 : E - d;
+  return E;
+}
+
 // --------------------------------------------------------------- integrals --
 // Scratch of the integral step: projections on the plane-pair lines of 5 vertices
 // and the 30 tets' values.

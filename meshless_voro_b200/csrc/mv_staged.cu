@@ -328,8 +328,10 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         __syncwarp();
       }
 
-      // ring of the removed region (compute_boundary + SimpleCycle iteration)
-      int E = ring_parallel<T>(S, lane, nvf, nv);
+      // ring of the removed region (compute_boundary + SimpleCycle iteration): lane e
+      // gets the boundary edge at ring position erank and creates its vertex
+      int eu = 0, ew = 0, erank = 0;
+      int E = ring_ranked<T>(S, lane, nvf, nv, &eu, &ew, &erank);
       if (E < 0) {
         WCNT(cc, ST_SERIAL_RING, 1);
         int e2 = 0;
@@ -341,11 +343,14 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           *err_code = MV_ERR_RING;
           return CELL_ERROR;
         }
+        if (lane < E) eu = S.ea[lane], ew = S.eb[lane];
+        erank = lane;
       }
       if (nvf + E > T::VMAX) return CELL_OVERFLOW;
       bool ok = true;
       double r2n = 0.0;
-      for (int ei = lane; ei < E; ei += 32)
+      if (lane < E) ok = make_vertex<PIdx>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
+      for (int ei = lane + 32; ei < E; ei += 32)  // rings of more than 32 edges (serial replay)
         ok &= make_vertex<PIdx>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
       if (__any_sync(FULL, !ok)) {
         *err_code = MV_ERR_DET;
