@@ -395,9 +395,10 @@ __device__ __noinline__ void sort_shell(ShellBuf<CMAX>& B, int lane, int n) {
   }
   __syncwarp();
   for (int k = 2; k <= np2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
+    for (int jl = __ffs(k) - 2; jl >= 0; jl--) {
+      const int j = 1 << jl;
       for (int i = lane; i < (np2 >> 1); i += 32) {
-        const int lo = 2 * j * (i / j) + (i % j);
+        const int lo = ((i >> jl) << (jl + 1)) | (i & (j - 1));
         const int hi = lo + j;
         const bool asc = (lo & k) == 0;
         const unsigned long long ka = B.key[lo], kb = B.key[hi];
@@ -624,10 +625,11 @@ __device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int
 
 // --------------------------------------------------------------- integrals --
 // Scratch of the integral step: projections on the plane-pair lines of 5 vertices
-// and the 30 tets' values.
+// and the 30 tets' values (rows padded so that lanes reading different rows at the
+// same column hit different banks).
 struct TetScratch {
   double ix[15], iy[15], iz[15];
-  double val[8][32];
+  double val[8][33];
 };
 
 // Integrals and face emission of a finished cell (convex_cell.rs:131-187,

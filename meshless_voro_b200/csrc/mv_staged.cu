@@ -36,6 +36,9 @@ constexpr int SHELL_CMAX = 128;
 constexpr int SHELL_WARPS = 4;
 constexpr int CLIP_WARPS = MV_CLIP_WARPS;
 constexpr int INT_WARPS = 4;
+#ifndef MV_INT_MINB
+#define MV_INT_MINB 8
+#endif
 using TierClip = Tier<64, 64, SHELL_CMAX, 8, uint8_t, MV_CLIP_MINB>;
 
 // Words of a cell record with np planes and nv vertices: header (np, nv), safety
@@ -485,7 +488,7 @@ struct RecordView {
 };
 
 template <class T, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) integrate_kernel(const __grid_constant__ Job J,
+__global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(const __grid_constant__ Job J,
                                                                const __grid_constant__ StageJob SJ) {
   __shared__ TetScratch scratch[WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
