@@ -10,9 +10,10 @@
 //   * the cell and face integrals (convex_cell.rs:131-187, voronoi_cell.rs:40-100,
 //     integrals.rs) over a read-only view of a finished cell.
 // Cell-state functions are templates over the shared-memory layout `SM`, which
-// provides the plane arrays pnx/pny/pnz/pd/ppx/ppy/ppz/pright/pcode/rptr and the
-// vertex arrays vx/vy/vz/vr2/f4/vd0/vd1/vd2/ord/ea/eb under those names (f4 holds the
-// f32 offset v - x of the filter; ord is 4-byte aligned).
+// provides the plane arrays pnx/pny/pnz/pd/pright/pcode/rptr, the vertex arrays
+// vx/vy/vz/vr2/f4/vd0/vd1/vd2/ord/ea/eb under those names (f4 holds the f32 offset
+// v - x of the filter; ord is 4-byte aligned) and plane_point(J, k), the point p of
+// boundary plane k.
 #pragma once
 #include <cstdint>
 
@@ -133,7 +134,7 @@ __device__ __forceinline__ D3 right_loc(const Job& J, const SM& S, int k, D3 x) 
     if (code != 13) l = add(l, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
     return l;
   }
-  D3 pr = plane_project({S.pnx[k], S.pny[k], S.pnz[k]}, {S.ppx[k], S.ppy[k], S.ppz[k]}, x);
+  D3 pr = plane_project({S.pnx[k], S.pny[k], S.pnz[k]}, S.plane_point(J, k), x);
   return sub(scale(2.0, pr), x);
 }
 

@@ -59,6 +59,7 @@ struct CellSmem {
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
   unsigned long long cnt[ST_COUNT];  // per-warp event counts (flushed to global at exit)
+  __device__ D3 plane_point(const Job&, int k) const { return {ppx[k], ppy[k], ppz[k]}; }
   union {
     struct {  // clipping phase
       ShellBuf<T::CMAX> sh;

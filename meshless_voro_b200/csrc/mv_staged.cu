@@ -94,9 +94,9 @@ __global__ void __launch_bounds__(32 * WARPS) shell_kernel(const __grid_constant
 template <class T>
 struct ClipSmem {
   using PIdx = typename T::PIdx;
-  // clipping planes (half_space.rs:9-19)
+  // clipping planes (half_space.rs:9-19); planes 0-5 are the boundary, the others
+  // bisectors whose point p = (x + ngb) / 2 is recomputed from the right generator
   double pnx[T::PMAX], pny[T::PMAX], pnz[T::PMAX], pd[T::PMAX];
-  double ppx[T::PMAX], ppy[T::PMAX], ppz[T::PMAX];
   int32_t pright[T::PMAX];  // original index of the right generator, -1: boundary
   uint8_t pcode[T::PMAX];   // periodic shift code, 13: none
   PIdx rptr[T::PMAX];       // ring successor (SimpleCycle::ptrs)
@@ -106,7 +106,13 @@ struct ClipSmem {
   alignas(4) PIdx ord[T::VMAX];   // position -> slot; [0, nv) is the reference's order
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
-  unsigned long long cnt[ST_COUNT];
+  // the window: 32 consecutive candidates of the list, as the reference sets them up
+  // (location, distance) plus the f32 operands and bound coefficients of the filter
+  double wgx[32], wgy[32], wgz[32], wdist[32];
+  float wex[32], wey[32], wez[32], wh[32], wc0[32], wc1[32];
+  int32_t worig[32];
+  uint8_t wcode[32];
+  __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
 };
 
 template <class T, int PREC>
@@ -119,7 +125,6 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   // ---- ConvexCell::init (convex_cell.rs:294-312) ----
   if (lane < 6) {
     S.pnx[lane] = J.bn[lane][0], S.pny[lane] = J.bn[lane][1], S.pnz[lane] = J.bn[lane][2];
-    S.ppx[lane] = J.bp[lane][0], S.ppy[lane] = J.bp[lane][1], S.ppz[lane] = J.bp[lane][2];
     S.pd[lane] = J.bd[lane];
     S.pright[lane] = -1;
     S.pcode[lane] = 13;
@@ -154,41 +159,43 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
     const bool valid = lane < wn;
     // candidate w0 + lane: location and offset as the reference computes them
     // (convex_cell.rs:333-342), plus the f32 quantities of the filter
-    D3 g = {0.0, 0.0, 0.0};
-    double dist = 1.0;
-    int orig = 0, code = 13;
-    float ex = 0.f, ey = 0.f, ez = 0.f, h = 0.f, c0 = 0.f, c1 = 0.f;
     bool bad = false, filt = false;
     if (valid) {
       const uint32_t pk = __ldg(list + w0 + lane);
       const int cp = (int)(pk / 27u);
-      code = (int)(pk - (uint32_t)cp * 27u);
-      g = {__ldg(J.sx + cp), __ldg(J.sy + cp), __ldg(J.sz + cp)};
-      orig = __ldg(J.sid + cp);
+      const int code = (int)(pk - (uint32_t)cp * 27u);
+      D3 g = {__ldg(J.sx + cp), __ldg(J.sy + cp), __ldg(J.sz + cp)};
+      const int orig = __ldg(J.sid + cp);
       if (code != 13) g = add(g, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
       const D3 dx = sub(x, g);
-      dist = sqrt(dot(dx, dx));
+      const double dist = sqrt(dot(dx, dx));
       bad = !(dist > 0.0 && dist <= DBL_MAX);
+      S.wgx[lane] = g.x, S.wgy[lane] = g.y, S.wgz[lane] = g.z, S.wdist[lane] = dist;
+      S.worig[lane] = orig;
+      S.wcode[lane] = (uint8_t)code;
       if (PREC == MV_PRECISION_FILTERED) {
         // s = e.a + |e|^2 / 2 is certified by T = c0 + c1 A with A >= |v - x| over the
         // cell's vertices (the bound of setup_batch, split into its A-free and A parts)
         filt = !bad && dist >= 1e-15 && dist <= 1e15 && x1 <= 1e15;
-        ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y), ez = __double2float_rn(dx.z);
-        h = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        const float ex = __double2float_rn(dx.x), ey = __double2float_rn(dx.y),
+                    ez = __double2float_rn(dx.z);
         const double e1 = fabs(dx.x) + fabs(dx.y) + fabs(dx.z);
         const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
         const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
         const double t0 = dist * (errb_up + u64 * (11.0 * e1 + 14.0 * x1) + u32 * (4.03 * dist));
-        c0 = __double2float_ru(t0 * (1.0 + 1e-6) + 1e-40);
-        c1 = __double2float_ru(dist * (u64 * 11.0 + u32 * 5.02) * (1.0 + 1e-6));
+        S.wex[lane] = ex, S.wey[lane] = ey, S.wez[lane] = ez;
+        S.wh[lane] = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        S.wc0[lane] = __double2float_ru(t0 * (1.0 + 1e-6) + 1e-40);
+        S.wc1[lane] = __double2float_ru(dist * (u64 * 11.0 + u32 * 5.02) * (1.0 + 1e-6));
       }
     }
+    __syncwarp();
     // window-constant ballots: degenerate distance, f32 filter applicable
     const unsigned mbad = __ballot_sync(FULL, valid && bad);
     unsigned mfilt = 0u;
     if (PREC == MV_PRECISION_FILTERED) mfilt = __ballot_sync(FULL, valid && filt && A32 <= 1e15f);
     // beyond the safety radius (refreshed when a clip shrinks it)
-    unsigned mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
+    unsigned mstop = __ballot_sync(FULL, valid && !bad && sr < S.wdist[lane]);
     // the f32 offset of this lane's vertex (position lane) for the filter
     float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
     if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
@@ -200,9 +207,8 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       if (PREC == MV_PRECISION_FILTERED) {
         // candidates certified to remove no vertex are consumed without their plane
         while (k < limit && ((mfilt >> k) & 1u)) {
-          const float exk = __shfl_sync(FULL, ex, k), eyk = __shfl_sync(FULL, ey, k);
-          const float ezk = __shfl_sync(FULL, ez, k), hk = __shfl_sync(FULL, h, k);
-          const float Tk = __fmaf_ru(__shfl_sync(FULL, c1, k), A32, __shfl_sync(FULL, c0, k));
+          const float exk = S.wex[k], eyk = S.wey[k], ezk = S.wez[k], hk = S.wh[k];
+          const float Tk = __fmaf_ru(S.wc1[k], A32, S.wc0[k]);
           bool need = lane < nv && !(fmaf(ezk, fv.z, fmaf(eyk, fv.y, fmaf(exk, fv.x, hk))) > Tk);
           if (nv > 32 && lane + 32 < nv) {
             const float4 f = S.f4[S.ord[lane + 32]];
@@ -225,17 +231,16 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const int e = k++;
       WCNT(cc, ST_NEIGHBOURS, 1);
       // ---- candidate e: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
-      const D3 ngb = shfl_d3(g, e);
-      const double de = __shfl_sync(FULL, dist, e);
-      const int orig_e = __shfl_sync(FULL, orig, e);
-      const int code_e = __shfl_sync(FULL, code, e);
+      const D3 ngb = {S.wgx[e], S.wgy[e], S.wgz[e]};
+      const double de = S.wdist[e];
+      const int orig_e = S.worig[e];
+      const int code_e = S.wcode[e];
       bool filt_e = false;
       float exe = 0.f, eye = 0.f, eze = 0.f, he = 0.f, Tk = 0.f;
       if (PREC == MV_PRECISION_FILTERED) {
         filt_e = (mfilt >> e) & 1u;
-        exe = __shfl_sync(FULL, ex, e), eye = __shfl_sync(FULL, ey, e);
-        eze = __shfl_sync(FULL, ez, e), he = __shfl_sync(FULL, h, e);
-        Tk = __fmaf_ru(__shfl_sync(FULL, c1, e), A32, __shfl_sync(FULL, c0, e));
+        exe = S.wex[e], eye = S.wey[e], eze = S.wez[e], he = S.wh[e];
+        Tk = __fmaf_ru(S.wc1[e], A32, S.wc0[e]);
       }
       const D3 dx = sub(x, ngb);
       const D3 n = divs(dx, de);
@@ -286,7 +291,6 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const int p_idx = np;
       if (lane == 0) {
         S.pnx[p_idx] = n.x, S.pny[p_idx] = n.y, S.pnz[p_idx] = n.z;
-        S.ppx[p_idx] = p.x, S.ppy[p_idx] = p.y, S.ppz[p_idx] = p.z;
         S.pd[p_idx] = d;
         S.pright[p_idx] = orig_e;
         S.pcode[p_idx] = (uint8_t)code_e;
@@ -370,7 +374,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         sr = 2.0 * sqrt(max_r2);
         A32 = amax32_of_sr(sr, dim);
       }
-      mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
+      mstop = __ballot_sync(FULL, valid && !bad && sr < S.wdist[lane]);
       if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
     }
   }
@@ -398,7 +402,17 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   uint8_t *d0 = pc + np, *d1 = d0 + nv, *d2 = d1 + nv;
   for (int pl = lane; pl < np; pl += 32) {
     const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
-    const D3 pr = plane_project(nn, {S.ppx[pl], S.ppy[pl], S.ppz[pl]}, x);
+    D3 pp;
+    const int rr = S.pright[pl];
+    if (rr < 0) {
+      pp = S.plane_point(J, pl);
+    } else {  // HalfSpace::new's p = (x + ngb) / 2, as at the clip
+      D3 ngb = load_gen(J, rr);
+      const int code = S.pcode[pl];
+      if (code != 13) ngb = add(ngb, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+      pp = scale(0.5, add(x, ngb));
+    }
+    const D3 pr = plane_project(nn, pp, x);
     nx[pl] = nn.x, ny[pl] = nn.y, nz[pl] = nn.z, dd[pl] = S.pd[pl];
     qx[pl] = pr.x, qy[pl] = pr.y, qz[pl] = pr.z;
     rt[pl] = S.pright[pl];
@@ -420,8 +434,9 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ClipSmem<T>& S = reinterpret_cast<ClipSmem<T>*>(smem_raw)[warp];
-  if (lane < ST_COUNT) S.cnt[lane] = 0ull;
-  __syncwarp();
+  __shared__ unsigned long long cnt[ST_COUNT];  // the block's event counts
+  if (threadIdx.x < ST_COUNT) cnt[threadIdx.x] = 0ull;
+  __syncthreads();
   for (;;) {
     int item = 0;
     if (lane == 0) item = (int)atomicAdd(SJ.work + 1, 1u);
@@ -452,7 +467,8 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
     if (lane == 0) {
       if (res == CELL_DONE) {
 #pragma unroll
-        for (int i = 0; i < ST_COUNT; i++) S.cnt[i] += cc.c[i];
+        for (int i = 0; i < ST_COUNT; i++)
+          if (cc.c[i]) atomicAdd(&cnt[i], (unsigned long long)cc.c[i]);
       } else {
         SJ.rec_off[item] = -1;
         if (res == CELL_ERROR) {
@@ -467,7 +483,8 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
     __syncwarp();
   }
   __syncwarp();
-  if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J.stats + lane, S.cnt[lane]);
+  __syncthreads();
+  if (threadIdx.x < ST_COUNT && cnt[threadIdx.x]) atomicAdd(J.stats + threadIdx.x, cnt[threadIdx.x]);
 }
 
 // --------------------------------------------------------------- integrals --
