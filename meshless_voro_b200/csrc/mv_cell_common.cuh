@@ -104,6 +104,13 @@ __device__ __forceinline__ int select_bit(const unsigned (&m)[NW], int s) {
   return -1;
 }
 
+// position of the s-th (1-based) set bit of a 64-bit mask
+__device__ __forceinline__ int select64(unsigned long long m, int s) {
+  const unsigned lo = (unsigned)m;
+  const int c = __popc(lo);
+  return s <= c ? (int)__fns(lo, 0, s) : 32 + (int)__fns((unsigned)(m >> 32), 0, s - c);
+}
+
 __device__ __forceinline__ unsigned valid_bits(int nv, int w) {
   const int lim = nv - 32 * w;
   return lim >= 32 ? FULL : (lim <= 0 ? 0u : ((1u << lim) - 1u));
@@ -416,6 +423,51 @@ __device__ __noinline__ void sort_shell(ShellBuf<CMAX>& B, int lane, int n) {
         }
       }
       __syncwarp();
+    }
+  }
+}
+
+// Bitonic sort of 32 * EPL shell entries held in registers, element i = lane + 32 e
+// in slot e of every lane: exchanges across lanes (stride < 32) go through warp
+// shuffles, exchanges inside a lane (stride >= 32) through registers, so the sort
+// touches no shared memory.  Entries order by (key, tie); (key, tie) pairs are
+// distinct except for the padding entries, which are identical.
+template <int EPL>
+__device__ __forceinline__ void sort_regs(unsigned long long (&key)[EPL], uint32_t (&tie)[EPL],
+                                          int32_t (&pos)[EPL], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * EPL; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int e = 0; e < EPL; e++) {
+          const int pe = e ^ (j >> 5);
+          if (pe > e) {
+            const bool asc = ((32 * e) & k) == 0;
+            const bool gt = key[e] > key[pe] || (key[e] == key[pe] && tie[e] > tie[pe]);
+            if (gt == asc) {
+              const unsigned long long tk = key[e];
+              const uint32_t tt = tie[e];
+              const int32_t tp = pos[e];
+              key[e] = key[pe], tie[e] = tie[pe], pos[e] = pos[pe];
+              key[pe] = tk, tie[pe] = tt, pos[pe] = tp;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < EPL; e++) {
+          const unsigned long long ok = __shfl_xor_sync(FULL, key[e], j);
+          const uint32_t ot = __shfl_xor_sync(FULL, tie[e], j);
+          const int32_t op = __shfl_xor_sync(FULL, pos[e], j);
+          const bool asc = (((lane + 32 * e) & k) == 0);
+          const bool lower = (lane & j) == 0;
+          const bool gt = key[e] > ok || (key[e] == ok && tie[e] > ot);  // mine > other
+          // the lower index of the pair keeps the smaller entry when ascending
+          if (gt == (lower == asc)) key[e] = ok, tie[e] = ot, pos[e] = op;
+        }
+      }
     }
   }
 }

@@ -34,6 +34,9 @@ namespace mv {
 #endif
 constexpr int SHELL_CMAX = 128;
 constexpr int SHELL_WARPS = 4;
+#ifndef MV_SHELL_MINB
+#define MV_SHELL_MINB 8
+#endif
 constexpr int CLIP_WARPS = MV_CLIP_WARPS;
 constexpr int INT_WARPS = 4;
 #ifndef MV_INT_MINB
@@ -49,8 +52,33 @@ __host__ __device__ __forceinline__ int64_t rec_words(int np, int nv) {
 }
 
 // ------------------------------------------------------------------- shell --
+// Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
+// sorted position * 27 + shift code; returns whether the nearest entry is the
+// generator itself.
+template <int EPL>
+__device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, int lane, int cnt,
+                                               int self, uint32_t* out) {
+  unsigned long long key[EPL];
+  uint32_t tie[EPL];
+  int32_t pos[EPL];
+#pragma unroll
+  for (int e = 0; e < EPL; e++) {
+    const int i = lane + 32 * e;
+    key[e] = i < cnt ? B.key[i] : ~0ull;
+    tie[e] = i < cnt ? B.tie[i] : ~0u;
+    pos[e] = i < cnt ? B.cpos[i] : 0;
+  }
+  sort_regs<EPL>(key, tie, pos, lane);
+#pragma unroll
+  for (int e = 0; e < EPL; e++) {
+    const int i = lane + 32 * e;
+    if (i < cnt) out[i] = (uint32_t)pos[e] * 27u + tie[e] % 27u;
+  }
+  return (int)(__shfl_sync(FULL, tie[0], 0) / 27u) == self;
+}
+
 template <int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) shell_kernel(const __grid_constant__ Job J,
+__global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const __grid_constant__ Job J,
                                                            const __grid_constant__ StageJob SJ) {
   __shared__ ShellBuf<SHELL_CMAX> bufs[WARPS];
   __shared__ double ext_s[6];
@@ -76,16 +104,17 @@ __global__ void __launch_bounds__(32 * WARPS) shell_kernel(const __grid_constant
       if (lane == 0) SJ.info[item] = -1;
       continue;
     }
-    sort_shell<SHELL_CMAX>(B, lane, cnt);
+    uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
+    bool self_first;
+    if (cnt <= 32)
+      self_first = sort_and_write<1>(B, lane, cnt, self, out);
+    else if (cnt <= 64)
+      self_first = sort_and_write<2>(B, lane, cnt, self, out);
+    else
+      self_first = sort_and_write<4>(B, lane, cnt, self, out);
     // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
     // fused kernel reports the error otherwise
-    if ((int)(B.tie[0] / 27u) != self) {
-      if (lane == 0) SJ.info[item] = -1;
-      continue;
-    }
-    uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
-    for (int k = lane; k < cnt; k += 32) out[k] = (uint32_t)B.cpos[k] * 27u + B.tie[k] % 27u;
-    if (lane == 0) SJ.info[item] = cnt | (all ? (1 << 30) : 0);
+    if (lane == 0) SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
     __syncwarp();
   }
 }
@@ -109,7 +138,8 @@ struct ClipSmem {
   // the window: 32 consecutive candidates of the list, as the reference sets them up
   // (location, distance) plus the f32 operands and bound coefficients of the filter
   double wgx[32], wgy[32], wgz[32], wdist[32];
-  float wex[32], wey[32], wez[32], wh[32], wc0[32], wc1[32];
+  float4 wf[32];  // filter operands: e = x - ngb in f32, |e|^2 / 2
+  float2 wc[32];  // bound coefficients (c0, c1)
   int32_t worig[32];
   uint8_t wcode[32];
   __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
@@ -119,6 +149,7 @@ template <class T, int PREC>
 __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int lane, int item,
                          int self, int info, int* err_code, CellCount& cc) {
   using PIdx = typename T::PIdx;
+  static_assert(T::NW == 2, "the swap-remove permutation uses 64-bit position masks");
   const D3 x = load_gen(J, self);
   const int dim = J.dim;
 
@@ -183,10 +214,9 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         const double u32 = 5.9604644775390625e-08, u64 = 1.1102230246251565e-16;
         const double errb_up = 1e-13 * (1.0 + 1.001 * (x1 + e1)) * 1.0001;
         const double t0 = dist * (errb_up + u64 * (11.0 * e1 + 14.0 * x1) + u32 * (4.03 * dist));
-        S.wex[lane] = ex, S.wey[lane] = ey, S.wez[lane] = ez;
-        S.wh[lane] = 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-        S.wc0[lane] = __double2float_ru(t0 * (1.0 + 1e-6) + 1e-40);
-        S.wc1[lane] = __double2float_ru(dist * (u64 * 11.0 + u32 * 5.02) * (1.0 + 1e-6));
+        S.wf[lane] = make_float4(ex, ey, ez, 0.5f * fmaf(ez, ez, fmaf(ey, ey, ex * ex)));
+        S.wc[lane] = make_float2(__double2float_ru(t0 * (1.0 + 1e-6) + 1e-40),
+                                 __double2float_ru(dist * (u64 * 11.0 + u32 * 5.02) * (1.0 + 1e-6)));
       }
     }
     __syncwarp();
@@ -207,8 +237,10 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       if (PREC == MV_PRECISION_FILTERED) {
         // candidates certified to remove no vertex are consumed without their plane
         while (k < limit && ((mfilt >> k) & 1u)) {
-          const float exk = S.wex[k], eyk = S.wey[k], ezk = S.wez[k], hk = S.wh[k];
-          const float Tk = __fmaf_ru(S.wc1[k], A32, S.wc0[k]);
+          const float4 fk = S.wf[k];
+          const float2 ck = S.wc[k];
+          const float exk = fk.x, eyk = fk.y, ezk = fk.z, hk = fk.w;
+          const float Tk = __fmaf_ru(ck.y, A32, ck.x);
           bool need = lane < nv && !(fmaf(ezk, fv.z, fmaf(eyk, fv.y, fmaf(exk, fv.x, hk))) > Tk);
           if (nv > 32 && lane + 32 < nv) {
             const float4 f = S.f4[S.ord[lane + 32]];
@@ -239,8 +271,10 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       float exe = 0.f, eye = 0.f, eze = 0.f, he = 0.f, Tk = 0.f;
       if (PREC == MV_PRECISION_FILTERED) {
         filt_e = (mfilt >> e) & 1u;
-        exe = S.wex[e], eye = S.wey[e], eze = S.wez[e], he = S.wh[e];
-        Tk = __fmaf_ru(S.wc1[e], A32, S.wc0[e]);
+        const float4 fe = S.wf[e];
+        const float2 ce = S.wc[e];
+        exe = fe.x, eye = fe.y, eze = fe.z, he = fe.w;
+        Tk = __fmaf_ru(ce.y, A32, ce.x);
       }
       const D3 dx = sub(x, ngb);
       const D3 n = divs(dx, de);
@@ -257,7 +291,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           const int sl = S.ord[q];
           bool decided = false;
           if (PREC == MV_PRECISION_FILTERED && filt_e) {
-            const float4 f = S.f4[sl];
+            const float4 f = w == 0 ? fv : S.f4[sl];  // position lane: held in registers
             const float s = fmaf(eze, f.z, fmaf(eye, f.y, fmaf(exe, f.x, he)));
             if (fabsf(s) > Tk) {
               removed = s < 0.f;
@@ -299,41 +333,40 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       WCNT(cc, ST_PLANES, 1);
 
       // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
-      unsigned km[T::NW];
-      int totK = 0;
-#pragma unroll
-      for (int w = 0; w < T::NW; w++) {
-        km[w] = ~rm[w] & valid_bits(nv, w);
-        totK += __popc(km[w]);
-      }
+      // over 64-bit masks of removed / kept positions; kept vertices before nvf stay
+      const unsigned long long rm64 = ((unsigned long long)rm[1] << 32) | rm[0];
+      const unsigned long long km64 = ~rm64 & (nv >= 64 ? ~0ull : ((1ull << nv) - 1ull));
+      const int totK = __popcll(km64);
       const int nvf = totK;
       {
-        int dest[T::NW];
-        PIdx held[T::NW];
+        int dest[2];
+        PIdx held[2];
 #pragma unroll
-        for (int w = 0; w < T::NW; w++) {
+        for (int w = 0; w < 2; w++) {
           const int q = lane + 32 * w;
           int dd = -1;
           held[w] = 0;
           if (q < nv) {
-            held[w] = S.ord[q];
-            if (!((rm[w] >> lane) & 1u)) {
-              dd = q < nvf ? q : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, q));
+            const unsigned long long below = (1ull << q) - 1ull;
+            if (!((rm64 >> q) & 1ull)) {
+              if (q >= nvf) dd = select64(rm64, totK - __popcll(km64 & below));
             } else if (q <= nvf) {
-              const int t = rank_below<T::NW>(rm, q) + 1;
-              dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
+              const int t = __popcll(rm64 & below) + 1;
+              dd = ((t == 1) ? nv : select64(km64, totK - t + 2)) - 1;
             } else {
               dd = q - 1;
             }
+            if (dd >= 0) held[w] = S.ord[q];
           }
           dest[w] = dd;
         }
         __syncwarp();
 #pragma unroll
-        for (int w = 0; w < T::NW; w++)
+        for (int w = 0; w < 2; w++)
           if (dest[w] >= 0) S.ord[dest[w]] = held[w];
         __syncwarp();
       }
+      double mk = 0.0;  // largest squared radius of this lane's vertices
 
       // ring of the removed region (compute_boundary + SimpleCycle iteration): lane e
       // gets the boundary edge at ring position erank and creates its vertex
@@ -356,19 +389,24 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       if (nvf + E > T::VMAX) return CELL_OVERFLOW;
       bool ok = true;
       double r2n = 0.0;
-      if (lane < E) ok = make_vertex<PIdx>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
-      for (int ei = lane + 32; ei < E; ei += 32)  // rings of more than 32 edges (serial replay)
+      if (lane < E) {
+        ok = make_vertex<PIdx>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
+        mk = fmax(mk, r2n);
+      }
+      for (int ei = lane + 32; ei < E; ei += 32) {  // rings of more than 32 edges (serial replay)
         ok &= make_vertex<PIdx>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
+        mk = fmax(mk, r2n);
+      }
       if (__any_sync(FULL, !ok)) {
         *err_code = MV_ERR_DET;
         return CELL_ERROR;
       }
       __syncwarp();
       nv = nvf + E;
-      // update_safety_radius (convex_cell.rs:443-453)
-      double m = 0.0;
-      for (int q = lane; q < nv; q += 32) m = fmax(m, S.vr2[S.ord[q]]);
-      const double mr = warp_max_nonneg(m);
+      // update_safety_radius (convex_cell.rs:443-453): the maximum over the kept and the
+      // new vertices
+      for (int q = lane; q < nvf; q += 32) mk = fmax(mk, S.vr2[S.ord[q]]);
+      const double mr = warp_max_nonneg(mk);
       if (__double_as_longlong(mr) != __double_as_longlong(max_r2)) {
         max_r2 = mr;
         sr = 2.0 * sqrt(max_r2);
