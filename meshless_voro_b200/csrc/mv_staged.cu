@@ -145,9 +145,22 @@ struct ClipSmem {
   __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
 };
 
+// Event counts of one clipped cell in two warp-uniform registers: a = neighbours
+// (16 bits) | planes (8) | serial rings (8), b = f32-undecided tests (16) | exact tests
+// (16).  A cell of the clip tier consumes at most 127 neighbours and holds at most 64
+// planes and 64 vertices, so no field overflows.
+struct ClipCount {
+  unsigned a, b;
+  __device__ void neighbours(unsigned v) { a += v; }
+  __device__ void plane() { a += 1u << 16; }
+  __device__ void serial_ring() { a += 1u << 24; }
+  __device__ void undecided(unsigned v) { b += v; }
+  __device__ void exact(unsigned v) { b += v << 16; }
+};
+
 template <class T, int PREC>
 __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int lane, int item,
-                         int self, int info, int* err_code, CellCount& cc) {
+                         int self, int info, int* err_code, ClipCount& cc) {
   using PIdx = typename T::PIdx;
   static_assert(T::NW == 2, "the swap-remove permutation uses 64-bit position masks");
   const D3 x = load_gen(J, self);
@@ -250,7 +263,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           k++;
         }
       }
-      WCNT(cc, ST_NEIGHBOURS, k - k0);
+      cc.neighbours(k - k0);
       if (k == limit) {
         if (limit == wn) break;  // window consumed
         if ((mbad >> k) & 1u) {
@@ -261,7 +274,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         break;
       }
       const int e = k++;
-      WCNT(cc, ST_NEIGHBOURS, 1);
+      cc.neighbours(1);
       // ---- candidate e: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
       const D3 ngb = {S.wgx[e], S.wgy[e], S.wgz[e]};
       const double de = S.wdist[e];
@@ -313,8 +326,8 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       }
       n_und = (int)__reduce_add_sync(FULL, (unsigned)n_und);
       n_ex = (int)__reduce_add_sync(FULL, (unsigned)n_ex);
-      if (PREC == MV_PRECISION_FILTERED) WCNT(cc, ST_F32_UNDECIDED, n_und);
-      WCNT(cc, ST_EXACT, n_ex);
+      if (PREC == MV_PRECISION_FILTERED) cc.undecided(n_und);
+      cc.exact(n_ex);
       int nrem = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
@@ -330,7 +343,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         S.pcode[p_idx] = (uint8_t)code_e;
       }
       np++;
-      WCNT(cc, ST_PLANES, 1);
+      cc.plane();
 
       // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
       // over 64-bit masks of removed / kept positions; kept vertices before nvf stay
@@ -373,7 +386,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       int eu = 0, ew = 0, erank = 0;
       int E = ring_ranked<T>(S, lane, nvf, nv, &eu, &ew, &erank);
       if (E < 0) {
-        WCNT(cc, ST_SERIAL_RING, 1);
+        cc.serial_ring();
         int e2 = 0;
         if (lane == 0) e2 = ring_serial<T>(S, nvf, nv, np);
         E = __shfl_sync(FULL, e2, 0);
@@ -497,16 +510,17 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
     const int info = SJ.info[item];
     int res = CELL_RETRY;
     int err = 0;
-    CellCount cc;
-#pragma unroll
-    for (int i = 0; i < ST_COUNT; i++) cc.c[i] = 0u;
+    ClipCount cc{0u, 0u};
     if (info > 0) res = clip_cell<T, PREC>(J, SJ, S, lane, item, self, info, &err, cc);
     __syncwarp();
     if (lane == 0) {
       if (res == CELL_DONE) {
+        const unsigned v[5] = {cc.a & 0xffffu, (cc.a >> 16) & 0xffu, cc.a >> 24, cc.b & 0xffffu,
+                               cc.b >> 16};
+        const int slot[5] = {ST_NEIGHBOURS, ST_PLANES, ST_SERIAL_RING, ST_F32_UNDECIDED, ST_EXACT};
 #pragma unroll
-        for (int i = 0; i < ST_COUNT; i++)
-          if (cc.c[i]) atomicAdd(&cnt[i], (unsigned long long)cc.c[i]);
+        for (int i = 0; i < 5; i++)
+          if (v[i]) atomicAdd(&cnt[slot[i]], (unsigned long long)v[i]);
       } else {
         SJ.rec_off[item] = -1;
         if (res == CELL_ERROR) {
