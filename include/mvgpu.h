@@ -182,6 +182,57 @@ int mv_voronoi_build_partial(const double* generators, const uint8_t* mask, int6
 
 void mv_voronoi_free(mv_voronoi* v);
 
+/* ---- the convex cells themselves (VoronoiIntegrator, voronoi.rs:527-828) ----
+ *
+ * A cells build returns, besides the Voronoi result, every built ConvexCell
+ * (convex_cell.rs:53-60) as CSR arrays indexed by generator (inactive cells are
+ * empty): its clipping planes and its vertices in the reference's order.  With
+ * MV_CELLS_TETS it also returns the oriented tets that custom integrals consume
+ * (CellIntegral::collect(v0, v1, v2, gen), integrals.rs:24-36; the generator is every
+ * tet's apex), in the order compute_cell_integral / compute_face_integrals feed them
+ * (convex_cell.rs:583-664): per vertex the six tets of DecompositionWithoutFaces, or,
+ * with MV_CELLS_WITH_FACES, per face the fan of DecompositionWithFaces
+ * (convex_cell.rs:89-129).  MV_CELLS_WITH_FACES also returns the faces of
+ * ConvexCell::with_faces (convex_cell.rs:461-543): the planes holding at least one
+ * vertex, in plane order, each with its vertex indices sorted by sort_face_vertices.
+ * with_faces is 3D only: MV_CELLS_WITH_FACES in 1D or 2D returns MV_ERR_ARG (the
+ * reference panics).  Plane and vertex indices are local to their cell. */
+enum { MV_CELLS_TETS = 1, MV_CELLS_WITH_FACES = 2 };
+
+typedef struct mv_cells {
+  int64_t n_cells, n_planes, n_vertices, n_tets, n_faces, n_face_vertices;
+  int64_t* cell_plane_offset;   /* [n + 1]                                            */
+  double* plane_normal;         /* [P][3] HalfSpace normal (half_space.rs:9-19)       */
+  double* plane_point;          /* [P][3] HalfSpace point p                           */
+  int32_t* plane_right;         /* [P]    right generator, -1: boundary plane         */
+  uint8_t* plane_shift_code;    /* [P]    13: no shift, see mv_shift_from_code        */
+  int64_t* cell_vertex_offset;  /* [n + 1]                                            */
+  double* vertex_loc;           /* [V][3] in the reference's vertex order             */
+  int32_t* vertex_dual;         /* [V][3] the three planes meeting at the vertex      */
+  int64_t* cell_tet_offset;     /* [n + 1]  (MV_CELLS_TETS)                           */
+  double* tet_vertices;         /* [T][3][3] v0, v1, v2                               */
+  int32_t* tet_plane;           /* [T]    the plane of the tet's base face            */
+  int64_t* cell_face_offset;    /* [n + 1]  (MV_CELLS_WITH_FACES)                     */
+  int32_t* face_plane;          /* [Fc]   the face's plane                            */
+  int64_t* face_vertex_offset;  /* [Fc + 1] into face_vertices                        */
+  int32_t* face_vertices;       /* [sum]  vertex indices, counter-clockwise           */
+} mv_cells;
+
+/* Cells build with device inputs: the Voronoi result as mv_context_build_device and the
+ * cells as device pointers owned by the context (valid until its next build). */
+int mv_context_build_cells_device(mv_context* ctx, const double* d_generators,
+                                  const uint8_t* d_mask, int64_t n, const double anchor[3],
+                                  const double width[3], int dimensionality, int periodic,
+                                  const mv_options* opts, int cells_flags,
+                                  mv_device_voronoi* voronoi, mv_cells* cells);
+
+/* Cells build with host inputs: both results copied to the context's pinned host arena
+ * (valid until the next build on the context; owned by the context). */
+int mv_context_build_cells(mv_context* ctx, const double* generators, const uint8_t* mask,
+                           int64_t n, const double anchor[3], const double width[3],
+                           int dimensionality, int periodic, const mv_options* opts,
+                           int cells_flags, mv_voronoi** voronoi, mv_cells** cells);
+
 /* ---- build without allocating (no counterpart in the reference crate) ----
  *
  * For callers that cannot call cudaMalloc -- a host framework that has handed all

@@ -27,6 +27,9 @@ MV_PRECISION_FILTERED = 1
 MV_FACES_OWNED = 0
 MV_FACES_ALL = 1
 
+MV_CELLS_TETS = 1
+MV_CELLS_WITH_FACES = 2
+
 MV_PIPELINE_AUTO = 0
 MV_PIPELINE_STAGED = 1
 MV_PIPELINE_FUSED = 2
@@ -38,7 +41,8 @@ EXPORTED = (
     "mv_options_default", "mv_strerror", "mv_version", "mv_context_create",
     "mv_context_destroy", "mv_context_last_stats", "mv_context_build_device",
     "mv_context_build", "mv_voronoi_build", "mv_voronoi_build_partial", "mv_voronoi_free",
-    "mv_shift_from_code", "mv_voronoi_build_noalloc",
+    "mv_shift_from_code", "mv_voronoi_build_noalloc", "mv_context_build_cells_device",
+    "mv_context_build_cells",
 )
 
 
@@ -89,6 +93,19 @@ class HostVoronoi(C.Structure):
                 ("error_cell", C.c_int64), ("_owner", C.c_void_p)]
 
 
+class Cells(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in (
+        "n_cells", "n_planes", "n_vertices", "n_tets", "n_faces", "n_face_vertices")] + [
+        ("cell_plane_offset", C.c_void_p), ("plane_normal", C.c_void_p),
+        ("plane_point", C.c_void_p), ("plane_right", C.c_void_p),
+        ("plane_shift_code", C.c_void_p), ("cell_vertex_offset", C.c_void_p),
+        ("vertex_loc", C.c_void_p), ("vertex_dual", C.c_void_p),
+        ("cell_tet_offset", C.c_void_p), ("tet_vertices", C.c_void_p),
+        ("tet_plane", C.c_void_p), ("cell_face_offset", C.c_void_p),
+        ("face_plane", C.c_void_p), ("face_vertex_offset", C.c_void_p),
+        ("face_vertices", C.c_void_p)]
+
+
 _lib = None
 
 
@@ -137,6 +154,15 @@ def lib():
                                                C.c_int, C.POINTER(Options),
                                                C.POINTER(DeviceVoronoi), C.c_int64, C.c_int64]
         L.mv_voronoi_build_noalloc.restype = C.c_int
+        L.mv_context_build_cells_device.argtypes = [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, dp, dp, C.c_int, C.c_int,
+            C.POINTER(Options), C.c_int, C.POINTER(DeviceVoronoi), C.POINTER(Cells)]
+        L.mv_context_build_cells_device.restype = C.c_int
+        L.mv_context_build_cells.argtypes = [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, dp, dp, C.c_int, C.c_int,
+            C.POINTER(Options), C.c_int, C.POINTER(C.POINTER(HostVoronoi)),
+            C.POINTER(C.POINTER(Cells))]
+        L.mv_context_build_cells.restype = C.c_int
         _lib = L
     return _lib
 

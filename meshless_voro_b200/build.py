@@ -17,7 +17,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libmvgpu.so")
 
-SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu", "mv_staged.cu"]
+SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu", "mv_staged.cu", "mv_export.cu"]
 HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h", "mv_cell_common.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

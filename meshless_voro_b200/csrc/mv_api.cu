@@ -23,6 +23,17 @@ namespace mv {
 cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
 int cells_blocks_per_sm_fast(int precision);
 int cells_blocks_per_sm_large(int precision);
+// mv_export.cu
+void launch_export_count(const int32_t* sid, const int64_t* rec_off, const double* rec, int n,
+                         int flags, int64_t* rec_by_orig, int32_t* planes, int32_t* verts,
+                         int32_t* tets, int32_t* faces, int32_t* face_verts, cudaStream_t st);
+void launch_export_write(const Job& J, const int64_t* rec_by_orig, const double* rec, int n, int flags,
+                         const int64_t* plane_off, const int64_t* vert_off, const int64_t* tet_off,
+                         const int64_t* face_off, const int64_t* face_vert_base, double* plane_normal,
+                         double* plane_point, int32_t* plane_right, uint8_t* plane_code,
+                         double* vert_loc, int32_t* vert_dual, double* tet_v, int32_t* tet_plane,
+                         int32_t* face_plane, int64_t* face_vert_off, int32_t* face_verts,
+                         int64_t n_faces, int64_t n_face_verts, int32_t* status, cudaStream_t st);
 // mv_staged.cu
 cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st);
 int stage_blocks_per_sm(int kernel, int precision);
@@ -148,6 +159,9 @@ struct Workspace {
   DevBuf counters;
   // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
   DevBuf cand, cand_info, rec_off, rec, retry, stage_ctr;
+  // cell export: record per generator, per-cell sizes and offsets, the CSR arrays
+  DevBuf x_rec_by_orig, x_cnt, x_off;
+  DevBuf x_pn, x_pp, x_pr, x_pc, x_vl, x_vd, x_tv, x_tp, x_fp, x_fvo, x_fv;
 };
 
 }  // namespace
@@ -172,6 +186,10 @@ struct mv_context {
   void* host = nullptr;
   size_t host_cap = 0;
   mv_voronoi hv{};
+  // pinned host arena for the cells of mv_context_build_cells
+  void* host_cells = nullptr;
+  size_t host_cells_cap = 0;
+  mv_cells hc{};
 };
 
 namespace {
@@ -241,9 +259,13 @@ int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224
 // Cells the first shell does not decide are appended to the retry list; *n_retry
 // receives their number.
 int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& o, int64_t n,
-               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry, double ms_stage[3]) {
+               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry, double ms_stage[3],
+               unsigned long long* keep_records) {
   Workspace& W = ctx->ws;
-  const int64_t chunk = std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
+  // an export build keeps every cell's record: one chunk, and the record counter the
+  // fused kernel shares (keep_records)
+  const int64_t chunk = keep_records ? n
+                                     : std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
   const int64_t nchunks = (n + chunk - 1) / chunk;
   const int stride = stage_list_stride();
   int64_t wpc = std::max<int64_t>(record_words_per_cell(s.dim), (int64_t)ctx->rec_words_hint);
@@ -279,7 +301,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
     SJ.item0 = (int32_t)(c * chunk);
     SJ.nitems = (int32_t)std::min<int64_t>(chunk, n - c * chunk);
     SJ.work = reinterpret_cast<unsigned int*>(ctr + 1 + 3 * c);
-    SJ.rec_counter = ctr + 1 + 3 * c + 2;
+    SJ.rec_counter = keep_records ? keep_records : ctr + 1 + 3 * c + 2;
     const int64_t warps_needed = SJ.nitems;
     for (int k = 0; k < 3; k++) {
       const int wpb = 4;  // every stage kernel runs 4 warps per block
@@ -309,13 +331,95 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
     const int64_t items = std::min<int64_t>(chunk, n - c * chunk);
     need = std::max(need, (double)h[1 + 3 * c + 2] / (double)std::max<int64_t>(items, 1));
   }
-  if (need * 1.1 > (double)wpc) ctx->rec_words_hint = need * 1.2;
+  if (!keep_records && need * 1.1 > (double)wpc) ctx->rec_words_hint = need * 1.2;
+  return MV_OK;
+}
+
+// Cells export (mv_export.cu): records by generator, sizes, offsets, then the arrays.
+int export_cells(mv_context* ctx, const Job& J, int64_t n, int flags, cudaStream_t st,
+                 int64_t* launches, mv_cells* out) {
+  Workspace& W = ctx->ws;
+  const size_t N = (size_t)std::max<int64_t>(n, 1);
+  int e = 0;
+  e |= ensure(ctx, W.x_rec_by_orig, 8 * N);
+  e |= ensure(ctx, W.x_cnt, 4 * 5 * N);
+  e |= ensure(ctx, W.x_off, 8 * 5 * (N + 1));
+  if (e) return MV_ERR_OOM;
+  int32_t* cnt = P<int32_t>(W.x_cnt);
+  int64_t* off = P<int64_t>(W.x_off);
+  const int ni = (int)n;
+  launch_export_count(J.sid, J.rec_off, J.rec, ni, flags, P<int64_t>(W.x_rec_by_orig), cnt,
+                      cnt + N, cnt + 2 * N, cnt + 3 * N, cnt + 4 * N, st);
+  (*launches)++;
+  int64_t tot[5] = {0, 0, 0, 0, 0};
+  if (n > 0) {
+    for (int k = 0; k < 5; k++) {
+      scan_i32_to_i64(cnt + k * N, n, off + k * (N + 1), P<long long>(W.scan_tmp), st);
+      MV_CUDA(cudaMemcpyAsync(&tot[k], off + k * (N + 1) + n, 8, cudaMemcpyDeviceToHost, st));
+    }
+    *launches += 15;
+  } else {
+    MV_CUDA(cudaMemsetAsync(off, 0, 8 * 5 * (N + 1), st));
+  }
+  MV_CUDA(cudaStreamSynchronize(st));
+  const size_t P_ = (size_t)std::max<int64_t>(tot[0], 1), V = (size_t)std::max<int64_t>(tot[1], 1),
+               T = (size_t)std::max<int64_t>(tot[2], 1), Fc = (size_t)std::max<int64_t>(tot[3], 1),
+               FV = (size_t)std::max<int64_t>(tot[4], 1);
+  e = 0;
+  e |= ensure(ctx, W.x_pn, 24 * P_);
+  e |= ensure(ctx, W.x_pp, 24 * P_);
+  e |= ensure(ctx, W.x_pr, 4 * P_);
+  e |= ensure(ctx, W.x_pc, P_);
+  e |= ensure(ctx, W.x_vl, 24 * V);
+  e |= ensure(ctx, W.x_vd, 12 * V);
+  if (flags & MV_CELLS_TETS) e |= ensure(ctx, W.x_tv, 72 * T) | ensure(ctx, W.x_tp, 4 * T);
+  if (flags & MV_CELLS_WITH_FACES)
+    e |= ensure(ctx, W.x_fp, 4 * Fc) | ensure(ctx, W.x_fvo, 8 * (Fc + 1)) | ensure(ctx, W.x_fv, 4 * FV);
+  if (e) return MV_ERR_OOM;
+  DevCounters* C = P<DevCounters>(W.counters);
+  launch_export_write(J, P<int64_t>(W.x_rec_by_orig), J.rec, ni, flags, off, off + (N + 1),
+                      off + 2 * (N + 1), off + 3 * (N + 1), off + 4 * (N + 1), P<double>(W.x_pn),
+                      P<double>(W.x_pp), P<int32_t>(W.x_pr), P<uint8_t>(W.x_pc), P<double>(W.x_vl),
+                      P<int32_t>(W.x_vd), P<double>(W.x_tv), P<int32_t>(W.x_tp), P<int32_t>(W.x_fp),
+                      P<int64_t>(W.x_fvo), P<int32_t>(W.x_fv), tot[3], tot[4], C->status, st);
+  *launches += (flags & MV_CELLS_WITH_FACES) ? 2 : 1;
+  MV_CUDA(cudaGetLastError());
+  int32_t status[STATUS_WORDS];
+  MV_CUDA(cudaMemcpyAsync(status, C->status, sizeof(status), cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaStreamSynchronize(st));
+  if (status[STATUS_CODE]) return status[STATUS_CODE];
+  std::memset(out, 0, sizeof(*out));
+  out->n_cells = n;
+  out->n_planes = tot[0], out->n_vertices = tot[1];
+  out->n_tets = (flags & MV_CELLS_TETS) ? tot[2] : 0;
+  out->n_faces = (flags & MV_CELLS_WITH_FACES) ? tot[3] : 0;
+  out->n_face_vertices = (flags & MV_CELLS_WITH_FACES) ? tot[4] : 0;
+  out->cell_plane_offset = off;
+  out->plane_normal = P<double>(W.x_pn);
+  out->plane_point = P<double>(W.x_pp);
+  out->plane_right = P<int32_t>(W.x_pr);
+  out->plane_shift_code = P<uint8_t>(W.x_pc);
+  out->cell_vertex_offset = off + (N + 1);
+  out->vertex_loc = P<double>(W.x_vl);
+  out->vertex_dual = P<int32_t>(W.x_vd);
+  if (flags & MV_CELLS_TETS) {
+    out->cell_tet_offset = off + 2 * (N + 1);
+    out->tet_vertices = P<double>(W.x_tv);
+    out->tet_plane = P<int32_t>(W.x_tp);
+  }
+  if (flags & MV_CELLS_WITH_FACES) {
+    out->cell_face_offset = off + 3 * (N + 1);
+    out->face_plane = P<int32_t>(W.x_fp);
+    out->face_vertex_offset = P<int64_t>(W.x_fvo);
+    out->face_vertices = P<int32_t>(W.x_fv);
+  }
   return MV_OK;
 }
 
 int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mask, int64_t n,
                       const double* anchor, const double* width, int dim, int periodic,
-                      const mv_options* opts_in, mv_device_voronoi* out) {
+                      const mv_options* opts_in, mv_device_voronoi* out, int cells_flags = -1,
+                      mv_cells* cells_out = nullptr) {
   mv_options o;
   mv_options_default(&o);
   if (opts_in) o = *opts_in;
@@ -325,6 +429,10 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   if (o.face_mode != MV_FACES_OWNED && o.face_mode != MV_FACES_ALL) return MV_ERR_ARG;
   if (o.pipeline < MV_PIPELINE_AUTO || o.pipeline > MV_PIPELINE_FUSED || o.chunk_cells < 0)
     return MV_ERR_ARG;
+  const bool exporting = cells_flags >= 0;
+  if (exporting && (!cells_out || (cells_flags & ~(MV_CELLS_TETS | MV_CELLS_WITH_FACES))))
+    return MV_ERR_ARG;
+  if (exporting && (cells_flags & MV_CELLS_WITH_FACES) && dim != 3) return MV_ERR_ARG;  // with_faces: 3D
   Setup s;
   int rc = make_setup(n, anchor, width, dim, periodic, o, &s);
   if (rc) return rc;
@@ -458,12 +566,25 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.stats = C->stats;
     const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
     const bool staged = use_staged(o, n);
+    if (exporting) {
+      // every built cell leaves a record: the staged clip kernel and the fused kernel
+      // (retries, small builds, the large tier) write them to one buffer
+      int64_t wpc = std::max<int64_t>(record_words_per_cell(s.dim), (int64_t)ctx->rec_words_hint);
+      const int64_t cap = (int64_t)N * wpc;
+      if (ensure(ctx, W.rec_off, 8 * N) || ensure(ctx, W.rec, 8 * (size_t)cap)) return MV_ERR_OOM;
+      MV_CUDA(cudaMemsetAsync(W.rec_off.p, 0xff, 8 * N, st));
+      J.rec = P<double>(W.rec);
+      J.rec_cap = (int64_t)(W.rec.cap / 8);
+      J.rec_counter = &C->rec_counter;
+      J.rec_off = P<int64_t>(W.rec_off);
+    }
     bool retry_ran = false;
     int64_t n_retry = 0;
     double ms_stage[3] = {0.0, 0.0, 0.0};
     MV_CUDA(cudaEventRecord(ctx->ev[1], st));
     if (n > 0 && staged) {
-      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry, ms_stage);
+      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry, ms_stage,
+                           exporting ? &C->rec_counter : nullptr);
       if (rc2) return rc2;
       MV_CUDA(cudaEventRecord(ctx->ev[2], st));
       if (n_retry > 0) {
@@ -524,6 +645,12 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
       return hc.status[STATUS_CODE];
     }
     if (hc.ovf_count[1] > 0) return MV_ERR_CAPACITY;
+    if (hc.status[STATUS_REC_OVERFLOW]) {
+      // the cell records did not fit: size the buffer from what was asked, rerun
+      if (attempt >= 2) return MV_ERR_CAPACITY;
+      ctx->rec_words_hint = 1.2 * (double)hc.rec_counter / (double)std::max<int64_t>(n, 1) + 8.0;
+      continue;
+    }
     if (hc.status[STATUS_FACE_OVERFLOW]) {
       if (attempt >= 2) return MV_ERR_CAPACITY;
       face_cap = (int64_t)(hc.face_counter * 1.15) + 4096;
@@ -581,6 +708,22 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   MV_CUDA(cudaEventRecord(ctx->ev[6], st));
   MV_CUDA(cudaGetLastError());
   MV_CUDA(cudaStreamSynchronize(st));
+  if (exporting) {
+    Job Jx;
+    std::memset(&Jx, 0, sizeof(Jx));
+    Jx.gen = P<double>(W.gen);
+    Jx.sid = P<int32_t>(W.sid);
+    for (int k = 0; k < 6; k++)
+      for (int i = 0; i < 3; i++) Jx.bp[k][i] = s.bp[k][i];
+    for (int c = 0; c < 27; c++) {
+      const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
+      for (int i = 0; i < 3; i++) Jx.shift[c][i] = -((double)(-m[i]) * s.width[i]);
+    }
+    Jx.rec = P<double>(W.rec);
+    Jx.rec_off = P<int64_t>(W.rec_off);
+    int rx = export_cells(ctx, Jx, n, cells_flags, st, &launches, cells_out);
+    if (rx) return rx;
+  }
   stats.device_bytes = (int64_t)ctx->dev_bytes;
   stats.kernel_launches = launches;
   {
@@ -697,9 +840,66 @@ int copy_to_host(mv_context* ctx, const mv_device_voronoi& d, int64_t n, const S
   return MV_OK;
 }
 
+// The cells of a cells build into the context's second pinned arena.
+int copy_cells_to_host(mv_context* ctx, const mv_cells& d, cudaStream_t st, mv_cells* h) {
+  const int64_t n = d.n_cells, P_ = d.n_planes, V = d.n_vertices, T = d.n_tets, Fc = d.n_faces,
+                FV = d.n_face_vertices;
+  const bool tets = d.tet_vertices != nullptr, faces = d.face_vertices != nullptr;
+  const size_t sz[] = {8 * (size_t)(n + 1), 24 * (size_t)P_, 24 * (size_t)P_, 4 * (size_t)P_,
+                       (size_t)P_, 8 * (size_t)(n + 1), 24 * (size_t)V, 12 * (size_t)V,
+                       tets ? 8 * (size_t)(n + 1) : 0, 72 * (size_t)T, 4 * (size_t)T,
+                       faces ? 8 * (size_t)(n + 1) : 0, 4 * (size_t)Fc,
+                       faces ? 8 * (size_t)(Fc + 1) : 0, 4 * (size_t)FV};
+  const int K = (int)(sizeof(sz) / sizeof(sz[0]));
+  size_t offs[16], total = 0;
+  for (int i = 0; i < K; i++) {
+    offs[i] = total;
+    total += (sz[i] + 255) & ~(size_t)255;
+  }
+  if (ctx->host_cells_cap < total) {
+    if (ctx->host_cells) cudaFreeHost(ctx->host_cells);
+    ctx->host_cells = nullptr;
+    ctx->host_cells_cap = 0;
+    const size_t want = total + total / 8 + 4096;
+    if (cudaHostAlloc(&ctx->host_cells, want, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->host_cells = nullptr;
+      return MV_ERR_OOM;
+    }
+    ctx->host_cells_cap = want;
+  }
+  char* b = static_cast<char*>(ctx->host_cells);
+  const void* src[] = {d.cell_plane_offset, d.plane_normal, d.plane_point, d.plane_right,
+                       d.plane_shift_code, d.cell_vertex_offset, d.vertex_loc, d.vertex_dual,
+                       d.cell_tet_offset, d.tet_vertices, d.tet_plane, d.cell_face_offset,
+                       d.face_plane, d.face_vertex_offset, d.face_vertices};
+  for (int i = 0; i < K; i++)
+    if (sz[i] && src[i]) MV_CUDA(cudaMemcpyAsync(b + offs[i], src[i], sz[i], cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaStreamSynchronize(st));
+  *h = d;
+  auto at = [&](int i, const void* p) -> char* { return p ? b + offs[i] : nullptr; };
+  h->cell_plane_offset = (int64_t*)at(0, d.cell_plane_offset);
+  h->plane_normal = (double*)at(1, d.plane_normal);
+  h->plane_point = (double*)at(2, d.plane_point);
+  h->plane_right = (int32_t*)at(3, d.plane_right);
+  h->plane_shift_code = (uint8_t*)at(4, d.plane_shift_code);
+  h->cell_vertex_offset = (int64_t*)at(5, d.cell_vertex_offset);
+  h->vertex_loc = (double*)at(6, d.vertex_loc);
+  h->vertex_dual = (int32_t*)at(7, d.vertex_dual);
+  h->cell_tet_offset = (int64_t*)at(8, d.cell_tet_offset);
+  h->tet_vertices = (double*)at(9, d.tet_vertices);
+  h->tet_plane = (int32_t*)at(10, d.tet_plane);
+  h->cell_face_offset = (int64_t*)at(11, d.cell_face_offset);
+  h->face_plane = (int32_t*)at(12, d.face_plane);
+  h->face_vertex_offset = (int64_t*)at(13, d.face_vertex_offset);
+  h->face_vertices = (int32_t*)at(14, d.face_vertices);
+  return MV_OK;
+}
+
 int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int64_t n,
                     const double* anchor, const double* width, int dim, int periodic,
-                    const mv_options* opts, mv_voronoi** out) {
+                    const mv_options* opts, mv_voronoi** out, int cells_flags = -1,
+                    mv_cells** cells_out = nullptr) {
   if (!ctx || !out || n < 0 || (n > 0 && !xyz)) return MV_ERR_ARG;
   mv_options o;
   mv_options_default(&o);
@@ -715,8 +915,10 @@ int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int
   if (mask && n > 0) MV_CUDA(cudaMemcpyAsync(ctx->ws.in_mask.p, mask, (size_t)n, cudaMemcpyHostToDevice, st));
   mv_device_voronoi d{};
   d.error_cell = -1;
+  mv_cells dc{};
   rc = build_device_impl(ctx, P<double>(ctx->ws.in_xyz), mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr,
-                         n, anchor, width, dim, periodic, &o, &d);
+                         n, anchor, width, dim, periodic, &o, &d, cells_flags,
+                         cells_flags >= 0 ? &dc : nullptr);
   if (rc) {
     std::memset(&ctx->hv, 0, sizeof(ctx->hv));
     ctx->hv.n_cells = n;
@@ -727,6 +929,11 @@ int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int
   rc = copy_to_host(ctx, d, n, s, st, &ctx->hv);
   if (rc) return rc;
   *out = &ctx->hv;
+  if (cells_flags >= 0) {
+    rc = copy_cells_to_host(ctx, dc, st, &ctx->hc);
+    if (rc) return rc;
+    *cells_out = &ctx->hc;
+  }
   return MV_OK;
 }
 
@@ -861,6 +1068,7 @@ void mv_context_destroy(mv_context* ctx) {
   for (size_t i = 0; i < nb; i++)
     if (bufs[i].p) cudaFree(bufs[i].p);
   if (ctx->host) cudaFreeHost(ctx->host);
+  if (ctx->host_cells) cudaFreeHost(ctx->host_cells);
   for (cudaEvent_t ev : ctx->stage_ev) cudaEventDestroy(ev);
   for (int i = 0; i < 10; i++)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -889,6 +1097,25 @@ int mv_context_build(mv_context* ctx, const double* generators, const uint8_t* m
   if (!anchor || !width) return MV_ERR_ARG;
   return build_host_impl(ctx, generators, mask, n, anchor, width, dimensionality, periodic, opts,
                          out);
+}
+
+int mv_context_build_cells_device(mv_context* ctx, const double* d_generators,
+                                  const uint8_t* d_mask, int64_t n, const double anchor[3],
+                                  const double width[3], int dimensionality, int periodic,
+                                  const mv_options* opts, int cells_flags,
+                                  mv_device_voronoi* voronoi, mv_cells* cells) {
+  if (!ctx || !anchor || !width || !cells || cells_flags < 0) return MV_ERR_ARG;
+  return build_device_impl(ctx, d_generators, d_mask, n, anchor, width, dimensionality, periodic,
+                           opts, voronoi, cells_flags, cells);
+}
+
+int mv_context_build_cells(mv_context* ctx, const double* generators, const uint8_t* mask,
+                           int64_t n, const double anchor[3], const double width[3],
+                           int dimensionality, int periodic, const mv_options* opts,
+                           int cells_flags, mv_voronoi** voronoi, mv_cells** cells) {
+  if (!anchor || !width || !cells || cells_flags < 0) return MV_ERR_ARG;
+  return build_host_impl(ctx, generators, mask, n, anchor, width, dimensionality, periodic, opts,
+                         voronoi, cells_flags, cells);
 }
 
 int mv_voronoi_build(const double* generators, int64_t n, const double anchor[3],

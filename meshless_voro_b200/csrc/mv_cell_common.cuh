@@ -219,7 +219,8 @@ enum CellResult {
   CELL_OVERFLOW = 1,
   CELL_ERROR = 2,
   CELL_FACE_OVERFLOW = 3,
-  CELL_RETRY = 4  // staged path: the cell needs the fused kernel (more neighbours)
+  CELL_RETRY = 4,  // staged path: the cell needs the fused kernel (more neighbours)
+  CELL_REC_OVERFLOW = 5  // export build: no room for the cell's record
 };
 
 // Event counts of one cell, kept in warp-uniform registers (a lane-0 branch inside
@@ -676,6 +677,100 @@ __device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int
   return E;
 }
 
+// ------------------------------------------------------------ cell records --
+// A finished cell as the staged integral kernel and the cell export read it, in words:
+// header (np, nv as int32), safety radius, plane normals / offsets / generator
+// projections (7 np f64), vertex locations in the reference's order (3 nv f64), right
+// generators (int32), plane shift codes and vertex duals (bytes).
+__host__ __device__ __forceinline__ int64_t rec_words(int np, int nv) {
+  return 2 + 7 * (int64_t)np + 3 * (int64_t)nv + (np + 1) / 2 + (np + 3 * nv + 7) / 8;
+}
+
+// Writes the cell held in shared memory (SM layout, see the top of this file, plus
+// bisector_point(J, k, x), the HalfSpace point p of plane k) as a record at words
+// allocated from *counter in rec[0, cap), and its offset to *off_slot.  Returns false
+// when the buffer is full or a plane index does not fit the record's bytes.
+template <class SM>
+__device__ bool write_record(const Job& J, double* rec, int64_t cap, unsigned long long* counter,
+                             int64_t* off_slot, const SM& S, int lane, D3 x, int np, int nv,
+                             double sr) {
+  if (np > 255) return false;
+  const int64_t words = rec_words(np, nv);
+  unsigned long long off = 0;
+  if (lane == 0) off = atomicAdd(counter, (unsigned long long)words);
+  off = __shfl_sync(FULL, off, 0);
+  if ((int64_t)off + words > cap) return false;
+  double* R = rec + off;
+  if (lane == 0) {
+    reinterpret_cast<int32_t*>(R)[0] = np;
+    reinterpret_cast<int32_t*>(R)[1] = nv;
+    R[1] = sr;
+  }
+  double* nx = R + 2;
+  double *ny = nx + np, *nz = ny + np, *dd = nz + np, *qx = dd + np, *qy = qx + np, *qz = qy + np;
+  double *vxo = qz + np, *vyo = vxo + nv, *vzo = vyo + nv;
+  int32_t* rt = reinterpret_cast<int32_t*>(vzo + nv);
+  uint8_t* pc = reinterpret_cast<uint8_t*>(vzo + nv + (np + 1) / 2);
+  uint8_t *d0 = pc + np, *d1 = d0 + nv, *d2 = d1 + nv;
+  for (int pl = lane; pl < np; pl += 32) {
+    const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
+    const D3 pr = plane_project(nn, S.bisector_point(J, pl, x), x);  // Plane::project_onto
+    nx[pl] = nn.x, ny[pl] = nn.y, nz[pl] = nn.z, dd[pl] = S.pd[pl];
+    qx[pl] = pr.x, qy[pl] = pr.y, qz[pl] = pr.z;
+    rt[pl] = S.pright[pl];
+    pc[pl] = S.pcode[pl];
+  }
+  for (int q = lane; q < nv; q += 32) {
+    const int sl = S.ord[q];
+    vxo[q] = S.vx[sl], vyo[q] = S.vy[sl], vzo[q] = S.vz[sl];
+    d0[q] = (uint8_t)S.vd0[sl], d1[q] = (uint8_t)S.vd1[sl], d2[q] = (uint8_t)S.vd2[sl];
+  }
+  if (lane == 0) *off_slot = (int64_t)off;
+  __syncwarp();
+  return true;
+}
+
+// The record at R as the integral step reads it (see integrate_view).
+struct RecordView {
+  const double *nx, *ny, *nz, *dd, *qx, *qy, *qz, *vx, *vy, *vz;
+  const int32_t* rt;
+  const uint8_t *pc, *d0, *d1, *d2;
+  int np, nv;
+  double sr;
+  __device__ explicit RecordView(const double* R) {
+    np = __ldg(reinterpret_cast<const int32_t*>(R));
+    nv = __ldg(reinterpret_cast<const int32_t*>(R) + 1);
+    sr = __ldg(R + 1);
+    nx = R + 2, ny = nx + np, nz = ny + np, dd = nz + np;
+    qx = dd + np, qy = qx + np, qz = qy + np;
+    vx = qz + np, vy = vx + nv, vz = vy + nv;
+    rt = reinterpret_cast<const int32_t*>(vz + nv);
+    pc = reinterpret_cast<const uint8_t*>(vz + nv + (np + 1) / 2);
+    d0 = pc + np, d1 = d0 + nv, d2 = d1 + nv;
+  }
+  __device__ D3 normal(int pl) const { return {__ldg(nx + pl), __ldg(ny + pl), __ldg(nz + pl)}; }
+  __device__ double d(int pl) const { return __ldg(dd + pl); }
+  __device__ D3 proj(int pl) const { return {__ldg(qx + pl), __ldg(qy + pl), __ldg(qz + pl)}; }
+  __device__ int right(int pl) const { return __ldg(rt + pl); }
+  __device__ int code(int pl) const { return __ldg(pc + pl); }
+  __device__ int dual(int q, int i) const {
+    return i == 0 ? __ldg(d0 + q) : (i == 1 ? __ldg(d1 + q) : __ldg(d2 + q));
+  }
+  __device__ D3 loc(int q) const { return {__ldg(vx + q), __ldg(vy + q), __ldg(vz + q)}; }
+};
+
+// Projection of x on the line of planes dual[i] & dual[i+1] of vertex q:
+// project_onto_intersection (geometry.rs:41-47) of plane dual[(i+1)%3] with dual[i].
+template <class View>
+__device__ __forceinline__ bool line_projection(const View& V, int q, int i, D3 x, D3* out) {
+  const int cur = V.dual(q, i);
+  const int nx = V.dual(q, i == 2 ? 0 : i + 1);
+  const D3 cn = V.normal(cur);
+  const D3 nn = V.normal(nx);
+  const D3 perp = cross(nn, cn);
+  return intersect3(nn, V.d(nx), cn, V.d(cur), perp, dot(x, perp), out);
+}
+
 // --------------------------------------------------------------- integrals --
 // Scratch of the integral step: projections on the plane-pair lines of 5 vertices
 // and the 30 tets' values (rows padded so that lanes reading different rows at the
@@ -709,14 +804,8 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
     bool ok = true;
     if (lane < 3 * nstep) {
       const int vl = lane / 3, i = lane - 3 * vl;
-      const int q = base + vl;
-      const int cur = V.dual(q, i);
-      const int nx = V.dual(q, i == 2 ? 0 : i + 1);
-      const D3 cn = V.normal(cur);
-      const D3 nn = V.normal(nx);
-      const D3 perp = cross(nn, cn);
       D3 pr = {0.0, 0.0, 0.0};
-      ok = intersect3(nn, V.d(nx), cn, V.d(cur), perp, dot(x, perp), &pr);
+      ok = line_projection(V, base + vl, i, x, &pr);
       Sc.ix[lane] = pr.x;
       Sc.iy[lane] = pr.y;
       Sc.iz[lane] = pr.z;

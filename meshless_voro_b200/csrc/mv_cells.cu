@@ -60,6 +60,7 @@ struct CellSmem {
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
   unsigned long long cnt[ST_COUNT];  // per-warp event counts (flushed to global at exit)
   __device__ D3 plane_point(const Job&, int k) const { return {ppx[k], ppy[k], ppz[k]}; }
+  __device__ D3 bisector_point(const Job&, int k, D3) const { return {ppx[k], ppy[k], ppz[k]}; }
   union {
     struct {  // clipping phase
       ShellBuf<T::CMAX> sh;
@@ -429,7 +430,11 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     // cell that is still open does not gather (and then shrink) a domain-wide shell
     R = fmin(fmax(R * 1.3, sr * 1.05), 2.0 * R);
   }
-  return integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
+  const int res = integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
+  if (res == CELL_DONE && J.rec != nullptr &&
+      !write_record(J, J.rec, J.rec_cap, J.rec_counter, J.rec_off + spos, S, lane, x, np, nv, sr))
+    return CELL_REC_OVERFLOW;
+  return res;
 }
 
 template <class T, int PREC, int WARPS>
@@ -480,6 +485,8 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
       }
     } else if (res == CELL_FACE_OVERFLOW) {
       if (lane == 0) atomicExch(J.status + STATUS_FACE_OVERFLOW, 1);
+    } else if (res == CELL_REC_OVERFLOW) {
+      if (lane == 0) atomicExch(J.status + STATUS_REC_OVERFLOW, 1);
     } else if (res == CELL_ERROR) {
       if (lane == 0) {
         atomicCAS(J.status + STATUS_CODE, 0, err);

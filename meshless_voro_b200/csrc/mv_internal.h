@@ -18,8 +18,10 @@ enum StatSlot {
 };
 
 // Device status words: [0] status code (first error wins), [1] failing cell (min),
-// [2] set when the face staging buffer was too small (the host grows it and reruns).
-enum { STATUS_CODE = 0, STATUS_CELL = 1, STATUS_FACE_OVERFLOW = 2, STATUS_WORDS = 4 };
+// [2] set when the face staging buffer was too small, [3] set when the cell-record
+// buffer of an export build was too small (the host grows the buffer and reruns).
+enum { STATUS_CODE = 0, STATUS_CELL = 1, STATUS_FACE_OVERFLOW = 2, STATUS_REC_OVERFLOW = 3,
+       STATUS_WORDS = 4 };
 
 // Device counters of one build (one allocation, cleared before each build).
 struct DevCounters {
@@ -32,6 +34,7 @@ struct DevCounters {
   unsigned int ovf_count[4];  // overflow lists of the capacity tiers
   int32_t bad_input;
   int32_t pad[3];
+  unsigned long long rec_counter;  // cell-record words allocated by an export build
 };
 
 // Face arrays (SoA; centroid and normal are [F][3]).
@@ -100,8 +103,14 @@ struct Job {
   unsigned int* work_counter;
   int32_t* ovf_list;        // cells that outgrew this capacity tier
   unsigned int* ovf_count;
-  int32_t* status;          // [2]
+  int32_t* status;          // [STATUS_WORDS]
   unsigned long long* stats;  // [ST_COUNT]
+  // ---- cell records of an export build (nullptr otherwise): the fused kernel writes
+  // the finished cells it builds, like the staged clip kernel ----
+  double* rec;
+  int64_t rec_cap;
+  unsigned long long* rec_counter;
+  int64_t* rec_off;         // by sorted position, -1: none
 };
 
 // One chunk of the staged path: cells at processing positions [item0, item0 + nitems)

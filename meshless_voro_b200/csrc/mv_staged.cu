@@ -44,13 +44,6 @@ constexpr int INT_WARPS = 4;
 #endif
 using TierClip = Tier<64, 64, SHELL_CMAX, 8, uint8_t, MV_CLIP_MINB>;
 
-// Words of a cell record with np planes and nv vertices: header (np, nv), safety
-// radius, plane normals / offsets / generator projections (7 np), vertex locations
-// (3 nv), right generators (int32) and plane codes + vertex duals (bytes).
-__host__ __device__ __forceinline__ int64_t rec_words(int np, int nv) {
-  return 2 + 7 * (int64_t)np + 3 * (int64_t)nv + (np + 1) / 2 + (np + 3 * nv + 7) / 8;
-}
-
 // ------------------------------------------------------------------- shell --
 // Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
 // sorted position * 27 + shift code; returns whether the nearest entry is the
@@ -143,6 +136,15 @@ struct ClipSmem {
   int32_t worig[32];
   uint8_t wcode[32];
   __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
+  // HalfSpace::p of plane k: the boundary point, or (x + ngb) / 2 recomputed as at the clip
+  __device__ D3 bisector_point(const Job& J, int k, D3 x) const {
+    const int rr = pright[k];
+    if (rr < 0) return plane_point(J, k);
+    D3 ngb = load_gen(J, rr);
+    const int code = pcode[k];
+    if (code != 13) ngb = add(ngb, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+    return scale(0.5, add(x, ngb));
+  }
 };
 
 // Event counts of one clipped cell in two warp-uniform registers: a = neighbours
@@ -434,48 +436,8 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   if (!finished && !(exhausted || sr < J.R0 * (1.0 - 1e-12))) return CELL_RETRY;
 
   // ---- the cell record for the integral kernel ----
-  const int64_t words = rec_words(np, nv);
-  unsigned long long off = 0;
-  if (lane == 0) off = atomicAdd(SJ.rec_counter, (unsigned long long)words);
-  off = __shfl_sync(FULL, off, 0);
-  if ((int64_t)off + words > SJ.rec_cap) return CELL_RETRY;
-  double* R = SJ.rec + off;
-  if (lane == 0) {
-    reinterpret_cast<int32_t*>(R)[0] = np;
-    reinterpret_cast<int32_t*>(R)[1] = nv;
-    R[1] = sr;
-  }
-  double* nx = R + 2;
-  double *ny = nx + np, *nz = ny + np, *dd = nz + np, *qx = dd + np, *qy = qx + np, *qz = qy + np;
-  double *vxo = qz + np, *vyo = vxo + nv, *vzo = vyo + nv;
-  int32_t* rt = reinterpret_cast<int32_t*>(vzo + nv);
-  uint8_t* pc = reinterpret_cast<uint8_t*>(vzo + nv + (np + 1) / 2);
-  uint8_t *d0 = pc + np, *d1 = d0 + nv, *d2 = d1 + nv;
-  for (int pl = lane; pl < np; pl += 32) {
-    const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
-    D3 pp;
-    const int rr = S.pright[pl];
-    if (rr < 0) {
-      pp = S.plane_point(J, pl);
-    } else {  // HalfSpace::new's p = (x + ngb) / 2, as at the clip
-      D3 ngb = load_gen(J, rr);
-      const int code = S.pcode[pl];
-      if (code != 13) ngb = add(ngb, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
-      pp = scale(0.5, add(x, ngb));
-    }
-    const D3 pr = plane_project(nn, pp, x);
-    nx[pl] = nn.x, ny[pl] = nn.y, nz[pl] = nn.z, dd[pl] = S.pd[pl];
-    qx[pl] = pr.x, qy[pl] = pr.y, qz[pl] = pr.z;
-    rt[pl] = S.pright[pl];
-    pc[pl] = S.pcode[pl];
-  }
-  for (int q = lane; q < nv; q += 32) {
-    const int sl = S.ord[q];
-    vxo[q] = S.vx[sl], vyo[q] = S.vy[sl], vzo[q] = S.vz[sl];
-    d0[q] = (uint8_t)S.vd0[sl], d1[q] = (uint8_t)S.vd1[sl], d2[q] = (uint8_t)S.vd2[sl];
-  }
-  if (lane == 0) SJ.rec_off[item] = (int64_t)off;
-  __syncwarp();
+  if (!write_record(J, SJ.rec, SJ.rec_cap, SJ.rec_counter, SJ.rec_off + item, S, lane, x, np, nv, sr))
+    return CELL_RETRY;
   return CELL_DONE;
 }
 
@@ -540,22 +502,6 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
 }
 
 // --------------------------------------------------------------- integrals --
-// A cell record as the integral step reads it.
-struct RecordView {
-  const double *nx, *ny, *nz, *dd, *qx, *qy, *qz, *vx, *vy, *vz;
-  const int32_t* rt;
-  const uint8_t *pc, *d0, *d1, *d2;
-  __device__ D3 normal(int pl) const { return {__ldg(nx + pl), __ldg(ny + pl), __ldg(nz + pl)}; }
-  __device__ double d(int pl) const { return __ldg(dd + pl); }
-  __device__ D3 proj(int pl) const { return {__ldg(qx + pl), __ldg(qy + pl), __ldg(qz + pl)}; }
-  __device__ int right(int pl) const { return __ldg(rt + pl); }
-  __device__ int code(int pl) const { return __ldg(pc + pl); }
-  __device__ int dual(int q, int i) const {
-    return i == 0 ? __ldg(d0 + q) : (i == 1 ? __ldg(d1 + q) : __ldg(d2 + q));
-  }
-  __device__ D3 loc(int q) const { return {__ldg(vx + q), __ldg(vy + q), __ldg(vz + q)}; }
-};
-
 template <class T, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(const __grid_constant__ Job J,
                                                                const __grid_constant__ StageJob SJ) {
@@ -572,19 +518,9 @@ __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(cons
     const int spos = SJ.item0 + item;
     const int self = __ldg(J.sid + spos);
     const D3 x = load_gen(J, self);
-    const double* R = SJ.rec + off;
-    const int np = __ldg(reinterpret_cast<const int32_t*>(R));
-    const int nv = __ldg(reinterpret_cast<const int32_t*>(R) + 1);
-    const double sr = __ldg(R + 1);
-    RecordView V;
-    V.nx = R + 2, V.ny = V.nx + np, V.nz = V.ny + np, V.dd = V.nz + np;
-    V.qx = V.dd + np, V.qy = V.qx + np, V.qz = V.qy + np;
-    V.vx = V.qz + np, V.vy = V.vx + nv, V.vz = V.vy + nv;
-    V.rt = reinterpret_cast<const int32_t*>(V.vz + nv);
-    V.pc = reinterpret_cast<const uint8_t*>(V.vz + nv + (np + 1) / 2);
-    V.d0 = V.pc + np, V.d1 = V.d0 + nv, V.d2 = V.d1 + nv;
+    const RecordView V(SJ.rec + off);
     int err = 0;
-    const int res = integrate_view<T>(J, V, scratch[warp], lane, self, x, nv, np, sr, &err);
+    const int res = integrate_view<T>(J, V, scratch[warp], lane, self, x, V.nv, V.np, V.sr, &err);
     if (res == CELL_DONE) {
       done++;
     } else if (lane == 0) {

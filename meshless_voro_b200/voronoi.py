@@ -122,6 +122,30 @@ class Context:
             raise N.MvError(rc, cell)
         return VoronoiArrays.from_host(out.contents, g, m, copy=True)
 
+    def build_cells(self, generators, mask, anchor, width, dimensionality, periodic,
+                    cells_flags=N.MV_CELLS_TETS, precision="filtered",
+                    face_mode=N.MV_FACES_OWNED, **kw):
+        """mv_context_build_cells: the Voronoi result and the built convex cells (host)."""
+        from .cells import CellsArrays
+        g = np.ascontiguousarray(np.asarray(generators, dtype=np.float64).reshape(-1, 3))
+        n = g.shape[0]
+        m = None
+        if mask is not None:
+            m = np.ascontiguousarray(np.asarray(mask, dtype=np.bool_).reshape(n)).view(np.uint8)
+        a, w = _vec3(anchor), _vec3(width)
+        opts = make_options(precision, face_mode, **kw)
+        hv = C.POINTER(N.HostVoronoi)()
+        hc = C.POINTER(N.Cells)()
+        rc = N.lib().mv_context_build_cells(self._h, g.ctypes.data_as(C.c_void_p),
+                                            m.ctypes.data_as(C.c_void_p) if m is not None else None,
+                                            n, _dp(a), _dp(w), int(dimensionality),
+                                            int(bool(periodic)), C.byref(opts), int(cells_flags),
+                                            C.byref(hv), C.byref(hc))
+        if rc != N.MV_OK:
+            cell = hv.contents.error_cell if hv else -1
+            raise N.MvError(rc, cell)
+        return VoronoiArrays.from_host(hv.contents, g, m, copy=True), CellsArrays.from_host(hc.contents)
+
     def build_device(self, d_generators: int, d_mask: int, n: int, anchor, width,
                      dimensionality, periodic, precision="filtered",
                      face_mode=N.MV_FACES_OWNED, stream=None, **kw) -> N.DeviceVoronoi:
@@ -341,38 +365,127 @@ class Voronoi:
 
 
 # ------------------------------------------------------------ integrals.rs --
+# The built-in integrals: the device computes them for every build; they also follow the
+# crate's protocol (init / collect / finalize over oriented tets), restated with glam's
+# operation order in binary64 (geometry.rs:82-100), for cells decomposed with faces.
+def _sub(a, b):
+    return (a[0] - b[0], a[1] - b[1], a[2] - b[2])
+
+
+def _dot(a, b):
+    return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]
+
+
+def _cross(a, b):
+    return (a[1] * b[2] - b[1] * a[2], a[2] * b[0] - b[2] * a[0], a[0] * b[1] - b[0] * a[1])
+
+
+def signed_volume_tet(v0, v1, v2, v3) -> float:
+    """geometry.rs:82-88: DMat3::from_cols(v1-v0, v2-v0, v3-v0).determinant() / 6"""
+    c0, c1, c2 = _sub(v1, v0), _sub(v2, v0), _sub(v3, v0)
+    return _dot(c2, _cross(c0, c1)) / 6.0
+
+
+def signed_area_tri(v0, v1, v2, t) -> float:
+    """geometry.rs:95-100"""
+    c = _cross(_sub(v1, v0), _sub(v2, v0))
+    n = (0.5 * c[0], 0.5 * c[1], 0.5 * c[2])
+    sign = np.copysign(1.0, _dot(_sub(t, v0), n))
+    return float(np.sqrt(_dot(n, n))) * float(sign)
+
+
+def _f3(v):
+    return (float(v[0]), float(v[1]), float(v[2]))
+
+
 class VolumeIntegral:
     """integrals.rs:124-142"""
     __slots__ = ("volume",)
 
-    def __init__(self, volume):
+    def __init__(self, volume=0.0):
         self.volume = volume
+
+    @classmethod
+    def init(cls, cell):
+        return cls(0.0)
+
+    def collect(self, v0, v1, v2, gen):
+        self.volume += signed_volume_tet(_f3(v0), _f3(v1), _f3(v2), _f3(gen))
+
+    def finalize(self):
+        return self
 
 
 class VolumeCentroidIntegral:
     """integrals.rs:69-106"""
     __slots__ = ("volume", "centroid")
 
-    def __init__(self, volume, centroid):
+    def __init__(self, volume=0.0, centroid=None):
         self.volume = volume
-        self.centroid = centroid
+        self.centroid = np.zeros(3) if centroid is None else centroid
+
+    @classmethod
+    def init(cls, cell):
+        return cls(0.0, (0.0, 0.0, 0.0))
+
+    def collect(self, v0, v1, v2, gen):
+        a, b, c, g = _f3(v0), _f3(v1), _f3(v2), _f3(gen)
+        vol = signed_volume_tet(a, b, c, g)
+        self.volume += vol
+        s = tuple(((a[i] + b[i]) + c[i]) + g[i] for i in range(3))
+        self.centroid = tuple(self.centroid[i] + vol * s[i] for i in range(3))
+
+    def finalize(self):
+        norm = 0.25 / self.volume if self.volume > 0.0 else 0.0
+        self.centroid = np.array([self.centroid[i] * norm for i in range(3)])
+        return self
 
 
 class AreaIntegral:
     """integrals.rs:343-361"""
     __slots__ = ("area",)
 
-    def __init__(self, area, centroid=None):
+    def __init__(self, area=0.0, centroid=None):
         self.area = area
+
+    @classmethod
+    def init(cls, cell, clipping_plane_idx):
+        return cls(0.0)
+
+    def collect(self, v0, v1, v2, gen):
+        self.area += signed_area_tri(_f3(v0), _f3(v1), _f3(v2), _f3(gen))
+
+    def finalize(self):
+        return self
 
 
 class AreaCentroidIntegral:
     """integrals.rs:283-320"""
     __slots__ = ("area", "centroid")
 
-    def __init__(self, area, centroid):
+    def __init__(self, area=0.0, centroid=None):
         self.area = area
-        self.centroid = centroid
+        self.centroid = np.zeros(3) if centroid is None else centroid
+
+    @classmethod
+    def init(cls, cell, clipping_plane_idx):
+        return cls(0.0, (0.0, 0.0, 0.0))
+
+    def collect(self, v0, v1, v2, gen):
+        a, b, c = _f3(v0), _f3(v1), _f3(v2)
+        ar = signed_area_tri(a, b, c, _f3(gen))
+        self.area += ar
+        s = tuple((a[i] + b[i]) + c[i] for i in range(3))
+        self.centroid = tuple(self.centroid[i] + ar * s[i] for i in range(3))
+
+    def finalize(self):
+        norm = 1.0 / (3.0 * self.area) if self.area > 0.0 else 0.0
+        self.centroid = np.array([self.centroid[i] * norm for i in range(3)])
+        return self
+
+
+_BUILTIN_CELL = (VolumeIntegral, VolumeCentroidIntegral)
+_BUILTIN_FACE = (AreaIntegral, AreaCentroidIntegral)
 
 
 class FaceIntegrator:
@@ -396,10 +509,13 @@ class FaceIntegrator:
 
 
 class VoronoiIntegrator:
-    """voronoi.rs:527-828 with the crate's built-in integrals evaluated on the GPU."""
+    """voronoi.rs:527-828: the built-in integrals come from the device build; custom
+    integrals (any class with the crate's init / collect / finalize protocol) and the
+    cells themselves come from a cells build (mv_context_build_cells), whose tets are
+    the reference's decomposition computed on the GPU."""
 
     def __init__(self, generators, mask, anchor, width, dimensionality, periodic, precision,
-                 context):
+                 context, with_faces=False):
         self._g = np.ascontiguousarray(np.asarray(generators, dtype=np.float64).reshape(-1, 3))
         self._mask = None if mask is None else np.asarray(mask, dtype=bool).reshape(-1)
         self._anchor, self._width = _vec3(anchor), _vec3(width)
@@ -407,6 +523,7 @@ class VoronoiIntegrator:
         self._periodic = bool(periodic)
         self._precision = precision
         self._ctx = context or default_context()
+        self._with_faces = with_faces
         self._cache = {}
 
     @staticmethod
@@ -415,6 +532,13 @@ class VoronoiIntegrator:
         return VoronoiIntegrator(generators, mask, anchor, width, dimensionality, periodic,
                                  precision, context)
 
+    def with_faces(self) -> "VoronoiIntegrator":
+        """voronoi.rs:621-638 / convex_cell.rs:461-466: 3D only (the crate panics)."""
+        if self._dim != 3:
+            raise ValueError("Can only convert to WithFaces in 3D!")
+        return VoronoiIntegrator(self._g, self._mask, self._anchor, self._width, self._dim,
+                                 self._periodic, self._precision, self._ctx, with_faces=True)
+
     def _run(self, face_mode) -> VoronoiArrays:
         if face_mode not in self._cache:
             self._cache[face_mode] = self._ctx.build_arrays(
@@ -422,19 +546,51 @@ class VoronoiIntegrator:
                 precision=self._precision, face_mode=face_mode)
         return self._cache[face_mode]
 
+    def _cells(self):
+        """(VoronoiArrays, CellsArrays) of a cells build (cached)."""
+        if "cells" not in self._cache:
+            flags = N.MV_CELLS_TETS | (N.MV_CELLS_WITH_FACES if self._with_faces else 0)
+            self._cache["cells"] = self._ctx.build_cells(
+                self._g, self._mask, self._anchor, self._width, self._dim, self._periodic,
+                cells_flags=flags, precision=self._precision)
+        return self._cache["cells"]
+
     def _active(self):
         n = self._g.shape[0]
         return np.ones(n, dtype=bool) if self._mask is None else self._mask
 
+    def cells_arrays(self):
+        """All built cells as CSR arrays (planes, vertices, tets, faces) for vectorised
+        custom integrals."""
+        return self._cells()[1]
+
+    def get_cell_at(self, index: int):
+        """voronoi.rs:647-649: the ConvexCell of a generator, None if it was not built."""
+        from .cells import ConvexCell
+        if not self._active()[index]:
+            return None
+        va, ca = self._cells()
+        return ConvexCell(ca, index, va.cell_loc[index], float(va.cell_safety_radius[index]),
+                          self._dim, self._width, self._with_faces)
+
+    def cells_iter(self) -> Iterator:
+        """voronoi.rs:655-657"""
+        for i in np.nonzero(self._active())[0]:
+            yield self.get_cell_at(int(i))
+
     def compute_cell_integrals(self, integral=VolumeCentroidIntegral):
         """voronoi.rs:668-673: one integral per active cell, in cell order."""
-        a = self._run(N.MV_FACES_OWNED)
-        idx = np.nonzero(self._active())[0]
-        if integral is VolumeIntegral:
-            return [VolumeIntegral(float(a.cell_volume[i])) for i in idx]
-        if integral is VolumeCentroidIntegral:
+        if integral in _BUILTIN_CELL and not self._with_faces:
+            a = self._run(N.MV_FACES_OWNED)
+            idx = np.nonzero(self._active())[0]
+            if integral is VolumeIntegral:
+                return [VolumeIntegral(float(a.cell_volume[i])) for i in idx]
             return [VolumeCentroidIntegral(float(a.cell_volume[i]), a.cell_centroid[i]) for i in idx]
-        raise NotImplementedError("custom cell integrals are not available on the device")
+        return [c.compute_cell_integral(integral) for c in self.cells_iter()]
+
+    def compute_cell_integrals_with_data(self, integral, extra_data):
+        """voronoi.rs:679-698"""
+        return [c.compute_cell_integral(integral, extra_data[c.idx]) for c in self.cells_iter()]
 
     def _faces(self, a: VoronoiArrays, integral):
         out = []
@@ -443,20 +599,38 @@ class VoronoiIntegrator:
             shift = shift_from_code(int(a.face_shift_code[f]), a.width)
             if integral is AreaIntegral:
                 val = AreaIntegral(float(a.face_area[f]))
-            elif integral is AreaCentroidIntegral:
-                val = AreaCentroidIntegral(float(a.face_area[f]), a.face_centroid[f])
             else:
-                raise NotImplementedError("custom face integrals are not available on the device")
+                val = AreaCentroidIntegral(float(a.face_area[f]), a.face_centroid[f])
             out.append(FaceIntegrator(int(a.face_left[f]), None if r < 0 else r, shift, val))
+        return out
+
+    def _custom_faces(self, integral, sym, extra_data=None):
+        mask = self._active()
+        out = []
+        for c in self.cells_iter():
+            data = None if extra_data is None else extra_data[c.idx]
+            out.extend(c.compute_face_integrals(integral, data, mask, sym))
         return out
 
     def compute_face_integrals(self, integral=AreaCentroidIntegral):
         """voronoi.rs:709-714: every face of every active cell (non-symmetric)."""
-        return self._faces(self._run(N.MV_FACES_ALL), integral)
+        if integral in _BUILTIN_FACE and not self._with_faces:
+            return self._faces(self._run(N.MV_FACES_ALL), integral)
+        return self._custom_faces(integral, sym=False)
 
     def compute_face_integrals_sym(self, integral=AreaCentroidIntegral):
         """voronoi.rs:725-732: each face once."""
-        return self._faces(self._run(N.MV_FACES_OWNED), integral)
+        if integral in _BUILTIN_FACE and not self._with_faces:
+            return self._faces(self._run(N.MV_FACES_OWNED), integral)
+        return self._custom_faces(integral, sym=True)
+
+    def compute_face_integrals_with_data(self, integral, extra_data):
+        """voronoi.rs:749-769"""
+        return self._custom_faces(integral, sym=False, extra_data=extra_data)
+
+    def compute_face_integrals_sym_with_data(self, integral, extra_data):
+        """voronoi.rs:784-808"""
+        return self._custom_faces(integral, sym=True, extra_data=extra_data)
 
     def to_voronoi(self) -> Voronoi:
         """From<&VoronoiIntegrator> for Voronoi (voronoi.rs:494-513)."""

@@ -876,6 +876,11 @@ struct OrcResult {
   std::vector<double> pl_n, pl_p, vx_loc;
   std::vector<int64_t> pl_right;
   std::vector<int32_t> pl_code, vx_dual;
+  // decomposition export (flag ORC_EXPORT_TETS; the fan tets with ORC_WITH_FACES) and
+  // sorted face-vertex lists (flag ORC_EXPORT_FACES)
+  std::vector<int64_t> tet_off, cf_off, fv_off;
+  std::vector<double> tet_v;
+  std::vector<int32_t> tet_plane, cf_plane, fv;
 };
 
 enum {
@@ -884,6 +889,8 @@ enum {
   ORC_BRUTE_FORCE = 4,    // one shell covering everything (checks the grid stream)
   ORC_EXPORT_CELLS = 8,   // keep planes/vertices of every built cell
   ORC_NO_CSR = 16,        // skip voronoi.rs finalize
+  ORC_EXPORT_TETS = 32,   // keep the decomposition tets of every built cell
+  ORC_EXPORT_FACES = 64,  // keep the with_faces vertex lists of every built cell
 };
 
 extern "C" {
@@ -921,6 +928,9 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
   bool export_cells = flags & ORC_EXPORT_CELLS;
   std::vector<std::vector<HalfSpace>> ex_planes(export_cells ? n : 0);
   std::vector<std::vector<Vertex>> ex_verts(export_cells ? n : 0);
+  const bool export_tets = flags & ORC_EXPORT_TETS, export_faces = flags & ORC_EXPORT_FACES;
+  std::vector<std::vector<Tet>> ex_tets(export_tets ? n : 0);
+  std::vector<FaceLists> ex_faces(export_faces ? n : 0);
   int status = 0;
   int64_t err_cell = -1;
 #ifdef _OPENMP
@@ -942,6 +952,19 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
       if (export_cells && !e) {
         ex_planes[k] = cell.planes;
         ex_verts[k] = cell.verts;
+      }
+      if ((export_tets || export_faces) && !e) {
+        FaceLists fl;
+        const bool fan = (flags & ORC_WITH_FACES) != 0;
+        if ((fan || export_faces) && !with_faces(cell, &fl)) e = ERR_DET;
+        if (!e && export_faces) ex_faces[k] = fl;
+        if (!e && export_tets) {
+          auto push = [&](const Tet& t) { ex_tets[k].push_back(t); };
+          if (fan)
+            decompose_with_faces(cell, fl, push);
+          else if (!decompose_without_faces(cell, push))
+            e = ERR_DET;
+        }
       }
       if (e) {
 #pragma omp critical
@@ -1023,7 +1046,44 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
       }
     }
   }
+  if (export_tets) {
+    R->tet_off.assign(n + 1, 0);
+    for (int64_t k = 0; k < n; k++) R->tet_off[k + 1] = R->tet_off[k] + (int64_t)ex_tets[k].size();
+    for (int64_t k = 0; k < n; k++)
+      for (const Tet& t : ex_tets[k]) {
+        R->tet_v.insert(R->tet_v.end(), {t.v0.x, t.v0.y, t.v0.z, t.v1.x, t.v1.y, t.v1.z, t.v2.x,
+                                         t.v2.y, t.v2.z});
+        R->tet_plane.push_back(t.plane);
+      }
+  }
+  if (export_faces) {
+    R->cf_off.assign(n + 1, 0);
+    for (int64_t k = 0; k < n; k++)
+      R->cf_off[k + 1] = R->cf_off[k] + (int64_t)ex_faces[k].plane.size();
+    R->fv_off.push_back(0);
+    for (int64_t k = 0; k < n; k++) {
+      const FaceLists& fl = ex_faces[k];
+      for (size_t f = 0; f < fl.plane.size(); f++) {
+        R->cf_plane.push_back(fl.plane[f]);
+        for (int i = 0; i < fl.count[f]; i++) R->fv.push_back(fl.verts[fl.offset[f] + i]);
+        R->fv_off.push_back((int64_t)R->fv.size());
+      }
+    }
+  }
   return R;
+}
+
+int64_t orc_n_tets_total(void* h) { return (int64_t)((OrcResult*)h)->tet_plane.size(); }
+int64_t orc_n_cell_faces_total(void* h) { return (int64_t)((OrcResult*)h)->cf_plane.size(); }
+int64_t orc_n_face_vertices_total(void* h) { return (int64_t)((OrcResult*)h)->fv.size(); }
+void orc_copy_tets(void* h, int64_t* tet_off, double* tet_v, int32_t* tet_plane) {
+  OrcResult* R = (OrcResult*)h;
+  cp(R->tet_off, tet_off), cp(R->tet_v, tet_v), cp(R->tet_plane, tet_plane);
+}
+void orc_copy_face_lists(void* h, int64_t* cf_off, int32_t* cf_plane, int64_t* fv_off,
+                         int32_t* fv) {
+  OrcResult* R = (OrcResult*)h;
+  cp(R->cf_off, cf_off), cp(R->cf_plane, cf_plane), cp(R->fv_off, fv_off), cp(R->fv, fv);
 }
 
 int orc_status(void* h) { return ((OrcResult*)h)->status; }

@@ -20,6 +20,8 @@ FACES_ALL = 1
 WITH_FACES = 2
 BRUTE_FORCE = 4
 EXPORT_CELLS = 8
+EXPORT_TETS = 32
+EXPORT_FACES = 64
 NO_CSR = 16
 
 STAT_FIELDS = ("n_nn", "n_planes", "n_vert", "max_vert", "n_exact", "n_shells", "n_cand", "pad")
@@ -49,6 +51,11 @@ def lib():
         L.orc_copy_conn.argtypes = [P, lp]
         L.orc_copy_stats.argtypes = [P, ip]
         L.orc_copy_cells_export.argtypes = [P, lp, dp, dp, lp, ip, lp, dp, ip]
+        for name in ("orc_n_tets_total", "orc_n_cell_faces_total", "orc_n_face_vertices_total"):
+            getattr(L, name).restype = C.c_int64
+            getattr(L, name).argtypes = [P]
+        L.orc_copy_tets.argtypes = [P, lp, dp, ip]
+        L.orc_copy_face_lists.argtypes = [P, lp, ip, lp, ip]
         L.orc_free.argtypes = [P]
         L.orc_signed_volume_tet.restype = C.c_double
         L.orc_signed_volume_tet.argtypes = [dp] * 4
@@ -164,6 +171,24 @@ def build(generators, anchor, width, dim=3, periodic=False, mask=None, nthreads=
             L.orc_copy_cells_export(h, _lp(ex["pl_off"]), _dp(ex["pl_n"]), _dp(ex["pl_p"]),
                                     _lp(ex["pl_right"]), _ip(ex["pl_code"]), _lp(ex["vx_off"]),
                                     _dp(ex["vx_loc"]), _ip(ex["vx_dual"]))
+            out.cells_export = ex
+        if flags & (EXPORT_TETS | EXPORT_FACES):
+            ex = out.cells_export if out.cells_export is not None else {}
+            if flags & EXPORT_TETS:
+                T = L.orc_n_tets_total(h)
+                ex["tet_off"] = np.zeros(n + 1, dtype=np.int64)
+                ex["tet_v"] = np.zeros((T, 3, 3))
+                ex["tet_plane"] = np.zeros(T, dtype=np.int32)
+                L.orc_copy_tets(h, _lp(ex["tet_off"]), _dp(ex["tet_v"]), _ip(ex["tet_plane"]))
+            if flags & EXPORT_FACES:
+                Fc = L.orc_n_cell_faces_total(h)
+                FV = L.orc_n_face_vertices_total(h)
+                ex["cf_off"] = np.zeros(n + 1, dtype=np.int64)
+                ex["cf_plane"] = np.zeros(Fc, dtype=np.int32)
+                ex["fv_off"] = np.zeros(Fc + 1, dtype=np.int64)
+                ex["fv"] = np.zeros(FV, dtype=np.int32)
+                L.orc_copy_face_lists(h, _lp(ex["cf_off"]), _ip(ex["cf_plane"]), _lp(ex["fv_off"]),
+                                      _ip(ex["fv"]))
             out.cells_export = ex
         return out
     finally:
