@@ -42,9 +42,17 @@ int64_t stage_record_words(int np, int nv);
 // mv_grid.cu
 void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
                  double* ext, int* bad, cudaStream_t st);
-void launch_grid(const double* gen, int n, const int G[3], const double a[3], const double inv[3],
-                 int32_t* cid, int32_t* count, int32_t* start, int32_t* fill, double* sx, double* sy,
-                 double* sz, int32_t* sid, long long* scan_tmp, cudaStream_t st);
+void launch_grid_coarse(const double* gen, int n, const int G[3], const double a[3],
+                        const double inv[3], int32_t* cid, int32_t* count, int32_t* start,
+                        int32_t* dflag, int32_t* dprefix, int32_t* cell_f, int32_t* fsize,
+                        int64_t* cell_fbase, int dim, long long* scan_tmp, cudaStream_t st);
+void launch_grid_fine(const double* gen, int n, const int G[3], const double a[3],
+                      const double inv[3], const int32_t* cid, const int32_t* start, int32_t* fill,
+                      const int32_t* cell_f, const int64_t* cell_fbase, int64_t nfine, int32_t* fid,
+                      int32_t* fine_cnt, int32_t* fine_pos, int32_t* fine_abs, double* sx, double* sy,
+                      double* sz, int32_t* sid, int dim, long long* scan_tmp, cudaStream_t st);
+void launch_scatter(const double* gen, int n, const int32_t* cid, const int32_t* start,
+                    int32_t* fill, double* sx, double* sy, double* sz, int32_t* sid, cudaStream_t st);
 size_t scan_tmp_elems(int64_t n);
 void scan_i32_to_i64(const int32_t* in, int64_t n, int64_t* out, long long* tmp, cudaStream_t st);
 void launch_reorder(const FaceArrays& stage, int64_t F, const int64_t* stage_off,
@@ -151,6 +159,7 @@ struct Workspace {
   DevBuf in_xyz, in_mask;
   DevBuf gen, sx, sy, sz, sid, cid;
   DevBuf cell_count, cell_start, cell_fill, scan_tmp;
+  DevBuf dflag, dprefix, cell_f, fsize, cell_fbase, fid, fine_cnt, fine_pos, fine_abs;
   DevBuf volume, centroid, sr, face_count, stage_off, face_off;
   DevBuf in_count, conn_count, conn_off, cursor, conn;
   DevBuf st_left, st_right, st_area, st_cen, st_nrm, st_code;
@@ -158,7 +167,7 @@ struct Workspace {
   DevBuf ovf_a, ovf_b;
   DevBuf counters;
   // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
-  DevBuf cand, cand_info, rec_off, rec, retry, stage_ctr;
+  DevBuf cand, cand_info, cand_rad, rec_off, rec, retry, stage_ctr;
   // cell export: record per generator, per-cell sizes and offsets, the CSR arrays
   DevBuf x_rec_by_orig, x_cnt, x_off;
   DevBuf x_pn, x_pp, x_pr, x_pc, x_vl, x_vd, x_tv, x_tp, x_fp, x_fvo, x_fv;
@@ -275,6 +284,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
   int e = 0;
   e |= ensure(ctx, W.cand, 4 * (size_t)chunk * stride);
   e |= ensure(ctx, W.cand_info, 4 * (size_t)chunk);
+  e |= ensure(ctx, W.cand_rad, 8 * (size_t)chunk);
   e |= ensure(ctx, W.rec_off, 8 * (size_t)chunk);
   e |= ensure(ctx, W.rec, 8 * (size_t)rec_cap);
   e |= ensure(ctx, W.retry, 4 * (size_t)n);
@@ -292,6 +302,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
   SJ.cstride = stride;
   SJ.cand = P<uint32_t>(W.cand);
   SJ.info = P<int32_t>(W.cand_info);
+  SJ.rad = P<double>(W.cand_rad);
   SJ.rec_off = P<int64_t>(W.rec_off);
   SJ.rec = P<double>(W.rec);
   SJ.rec_cap = rec_cap;
@@ -454,6 +465,12 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   e |= ensure(ctx, W.cell_count, 4 * (ncell + 1));
   e |= ensure(ctx, W.cell_start, 4 * (ncell + 1));
   e |= ensure(ctx, W.cell_fill, 4 * (ncell + 1));
+  e |= ensure(ctx, W.dflag, 4 * (ncell + 1));
+  e |= ensure(ctx, W.dprefix, 4 * (ncell + 1));
+  e |= ensure(ctx, W.cell_f, 4 * (ncell + 1));
+  e |= ensure(ctx, W.fsize, 4 * (ncell + 1));
+  e |= ensure(ctx, W.cell_fbase, 8 * (ncell + 1));
+  e |= ensure(ctx, W.fid, 4 * N);
   e |= ensure(ctx, W.scan_tmp, 8 * (scan_tmp_elems(std::max<int64_t>(ncell + 1, N)) + 64));
   e |= ensure(ctx, W.volume, 8 * N);
   e |= ensure(ctx, W.centroid, 24 * N);
@@ -498,12 +515,36 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
 
     // ---- generators + grid (replaces build_rtree, rtree_nn.rs:6-8) ----
     MV_CUDA(cudaEventRecord(ctx->ev[0], st));
-    launches = 7;  // prep, extent, cell index, 3 scan kernels, scatter
+    launches = 13;  // prep, extent, cell index, 3 x 3 scan kernels, dense flags, scatter
     launch_prep(d_xyz, ni, s.dim, P<double>(W.gen), C->ext_keys, C->ext, &C->bad_input, st);
-    launch_grid(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
-                P<int32_t>(W.cell_count), P<int32_t>(W.cell_start), P<int32_t>(W.cell_fill),
-                P<double>(W.sx), P<double>(W.sy), P<double>(W.sz), P<int32_t>(W.sid),
-                P<long long>(W.scan_tmp), st);
+    launch_grid_coarse(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
+                       P<int32_t>(W.cell_count), P<int32_t>(W.cell_start), P<int32_t>(W.dflag),
+                       P<int32_t>(W.dprefix), P<int32_t>(W.cell_f), P<int32_t>(W.fsize),
+                       P<int64_t>(W.cell_fbase), s.dim, P<long long>(W.scan_tmp), st);
+    int32_t ndense = 0;
+    int64_t nfine = 0;
+    MV_CUDA(cudaMemcpyAsync(&ndense, P<int32_t>(W.dprefix) + ncell, 4, cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaMemcpyAsync(&nfine, P<int64_t>(W.cell_fbase) + ncell, 8, cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+    if (ndense > 0) {
+      // clustered input: the dense cells get a second grid level
+      e = 0;
+      e |= ensure(ctx, W.fine_cnt, 4 * (size_t)nfine);
+      e |= ensure(ctx, W.fine_pos, 4 * (size_t)(nfine + 1));
+      e |= ensure(ctx, W.fine_abs, 4 * (size_t)nfine);
+      if (e) return MV_ERR_OOM;
+      launch_grid_fine(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
+                       P<int32_t>(W.cell_start), P<int32_t>(W.cell_fill), P<int32_t>(W.cell_f),
+                       P<int64_t>(W.cell_fbase), nfine, P<int32_t>(W.fid), P<int32_t>(W.fine_cnt),
+                       P<int32_t>(W.fine_pos), P<int32_t>(W.fine_abs), P<double>(W.sx),
+                       P<double>(W.sy), P<double>(W.sz), P<int32_t>(W.sid), s.dim,
+                       P<long long>(W.scan_tmp), st);
+      launches += 6;
+    } else {
+      launch_scatter(P<double>(W.gen), ni, P<int32_t>(W.cid), P<int32_t>(W.cell_start),
+                     P<int32_t>(W.cell_fill), P<double>(W.sx), P<double>(W.sy), P<double>(W.sz),
+                     P<int32_t>(W.sid), st);
+    }
 
     // ---- cells ----
     Job J;
@@ -514,6 +555,12 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.sz = P<double>(W.sz);
     J.sid = P<int32_t>(W.sid);
     J.cell_start = P<int32_t>(W.cell_start);
+    if (ndense > 0) {
+      J.dprefix = P<int32_t>(W.dprefix);
+      J.cell_f = P<int32_t>(W.cell_f);
+      J.cell_fbase = P<int64_t>(W.cell_fbase);
+      J.fine_abs = P<int32_t>(W.fine_abs);
+    }
     J.mask = d_mask;
     J.n = ni;
     J.dim = s.dim;
@@ -532,6 +579,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     J.ext = C->ext;
     J.R0 = s.R0;
+    J.ppc_mean = (double)std::max<int64_t>(n, 1) / (double)ncell;
     for (int c = 0; c < 27; c++) {
       const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
       for (int i = 0; i < 3; i++) {

@@ -231,6 +231,45 @@ struct CellCount {
 #define WCNT(CC, slot, v) ((CC).c[slot] += (unsigned)(v))
 
 // ------------------------------------------------------------- neighbour shell --
+// Radius of a cell's first shell: R0, scaled down in dense cells by the local density
+// (of the generator's sub-cell when it holds a few generators, else of its grid cell)
+// so that the first shell holds about as many candidates as in a uniform region.
+// Shells are prefixes of the same nearest-first stream, so the radius only moves work
+// between shells, never the result.
+__device__ __forceinline__ double first_radius(const Job& J, D3 x) {
+  if (J.cell_f == nullptr) return J.R0;
+  const double xa[3] = {x.x, x.y, x.z};
+  int c[3];
+  double t[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    t[i] = (xa[i] - J.ga[i]) * J.ginv[i];
+    double f = floor(t[i]);
+    if (!(f >= 0.0)) f = 0.0;
+    if (f > J.G[i] - 1) f = J.G[i] - 1;
+    c[i] = (int)f;
+  }
+  const int64_t cc = (int64_t)c[0] + (int64_t)J.G[0] * (c[1] + (int64_t)J.G[1] * c[2]);
+  const int f = __ldg(J.cell_f + cc);
+  if (f == 0) return J.R0;
+  const int cnt = __ldg(J.cell_start + cc + 1) - __ldg(J.cell_start + cc);
+  int q[3], fa[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    fa[i] = i < J.dim ? f : 1;
+    double u = floor((t[i] - (double)c[i]) * (double)fa[i]);
+    if (!(u >= 0.0)) u = 0.0;
+    if (u > fa[i] - 1) u = fa[i] - 1;
+    q[i] = (int)u;
+  }
+  const int64_t slot = __ldg(J.cell_fbase + cc) + q[0] + (int64_t)fa[0] * (q[1] + (int64_t)fa[1] * q[2]);
+  const int cf = __ldg(J.fine_abs + slot + 1) - __ldg(J.fine_abs + slot);
+  const double nsub = (double)fa[0] * fa[1] * fa[2];
+  const double ratio = cf >= 4 ? (double)cf * nsub / J.ppc_mean : (double)cnt / J.ppc_mean;
+  if (!(ratio > 1.0)) return J.R0;
+  return J.R0 * pow(ratio, -1.0 / J.dim);
+}
+
 template <int CMAX>
 struct ShellBuf {
   unsigned long long key[CMAX];  // f64 squared distance bits
@@ -247,6 +286,12 @@ struct ShellBuf {
 // ends with this shell.  d2 is the reference's squared distance:
 // (g - q).length_squared() for nn_iter (rstar) and |(q + s) - g|^2 for
 // wrapping_nn_iter (rtree_nn.rs:138-146).
+//
+// Grid rows (y, z) go to lanes; a lane turns the cells of its row that the ball
+// reaches into contiguous segments of sorted positions (one per periodic image).  A
+// segment that contains a dense cell (J.dprefix) is deferred: its cells are then
+// visited one by one, and a dense cell contributes the rows of its sub-grid that the
+// ball reaches.  Without the ball test (all images enumerated) every sub-cell counts.
 template <int CMAX>
 __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
                                          double lo2, const double* ext, bool* exhausted) {
@@ -271,80 +316,33 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
   const int nrows = ny * nz;
   int count = 0;
 
-  // box-distance of unwrapped grid coordinate u along axis i
-  auto box_d = [&](int i, int u) -> double {
-    int G = J.G[i];
-    bool wrap = J.periodic && i < J.dim;
-    int m = u < 0 ? -1 : (u >= G ? 1 : 0);
-    int c = u - m * G;
-    double blo = J.ga[i] + c * J.gh[i], bhi = J.ga[i] + (c + 1) * J.gh[i];
+  // bounds of coarse cell c (image m) along axis i, inflated against rounding; the
+  // edge cells reach the generators' extent (periodic) or infinity (rectangular)
+  auto cell_lo = [&](int i, int c, int m) -> double {
+    const bool wrap = J.periodic && i < J.dim;
+    double blo = J.ga[i] + c * J.gh[i];
     if (c == 0) blo = wrap ? fmin(blo, ext[i]) : -__longlong_as_double(0x7ff0000000000000ll);
-    if (c == G - 1) bhi = wrap ? fmax(bhi, ext[3 + i]) : __longlong_as_double(0x7ff0000000000000ll);
-    blo += m * J.gw[i] - J.geps[i];
-    bhi += m * J.gw[i] + J.geps[i];
+    return blo + m * J.gw[i] - J.geps[i];
+  };
+  auto cell_hi = [&](int i, int c, int m) -> double {
+    const bool wrap = J.periodic && i < J.dim;
+    double bhi = J.ga[i] + (c + 1) * J.gh[i];
+    if (c == J.G[i] - 1) bhi = wrap ? fmax(bhi, ext[3 + i]) : __longlong_as_double(0x7ff0000000000000ll);
+    return bhi + m * J.gw[i] + J.geps[i];
+  };
+  auto dist1 = [&](int i, double blo, double bhi) -> double {
     return xa[i] < blo ? blo - xa[i] : (xa[i] > bhi ? xa[i] - bhi : 0.0);
   };
+  // box-distance of unwrapped grid coordinate u along axis i
+  auto box_d = [&](int i, int u) -> double {
+    const int G = J.G[i];
+    const int m = u < 0 ? -1 : (u >= G ? 1 : 0);
+    const int c = u - m * G;
+    return dist1(i, cell_lo(i, c, m), cell_hi(i, c, m));
+  };
 
-  for (int row0 = 0; row0 < nrows; row0 += 32) {
-    const int row = row0 + lane;
-    int nseg = 0;
-    int32_t s0a = 0, s0b = 0, s0c = 0, sla = 0, slb = 0, slc = 0;
-    int sca = 0, scb = 0, scc = 0;
-    if (row < nrows) {
-      const int uy = lo[1] + row % ny, uz = lo[2] + row / ny;
-      const double dy = box_d(1, uy), dz = box_d(2, uz);
-      const double byz2 = dy * dy + dz * dz;
-      if (all || byz2 < R2v) {
-        int first = 1 << 30, last = -(1 << 30);
-        for (int ux = lo[0]; ux <= hi[0]; ux++) {
-          double dx = box_d(0, ux);
-          if (all || dx * dx + byz2 < R2v) {
-            first = min(first, ux);
-            last = max(last, ux);
-          }
-        }
-        const int Gx = J.G[0], Gy = J.G[1], Gz = J.G[2];
-        const int my = uy < 0 ? -1 : (uy >= Gy ? 1 : 0);
-        const int mz = uz < 0 ? -1 : (uz >= Gz ? 1 : 0);
-        const int cy = uy - my * Gy, cz = uz - mz * Gz;
-        const int64_t rowbase = (int64_t)Gx * (cy + (int64_t)Gy * cz);
-        for (int mx = -1; mx <= 1; mx++) {
-          int a = max(first, mx * Gx), b = min(last, mx * Gx + Gx - 1);
-          if (a > b) continue;
-          int c0 = a - mx * Gx, c1 = b - mx * Gx;
-          int32_t ps = __ldg(J.cell_start + rowbase + c0);
-          int32_t pe = __ldg(J.cell_start + rowbase + c1 + 1);
-          if (pe > ps) {
-            const int code = (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
-            if (nseg == 0) {
-              s0a = ps, sla = pe - ps, sca = code;
-            } else if (nseg == 1) {
-              s0b = ps, slb = pe - ps, scb = code;
-            } else {
-              s0c = ps, slc = pe - ps, scc = code;
-            }
-            nseg++;
-          }
-        }
-      }
-    }
-    int nsegs_total;
-    const int segoff = warp_excl_scan(nseg, lane, &nsegs_total);
-    const int mylen = sla + slb + slc;
-    int total;
-    const int lenoff = warp_excl_scan(mylen, lane, &total);
-    if (nseg > 0) {
-      B.sstart[segoff] = s0a, B.spref[segoff] = lenoff, B.scode[segoff] = (uint8_t)sca;
-    }
-    if (nseg > 1) {
-      B.sstart[segoff + 1] = s0b, B.spref[segoff + 1] = lenoff + sla;
-      B.scode[segoff + 1] = (uint8_t)scb;
-    }
-    if (nseg > 2) {
-      B.sstart[segoff + 2] = s0c, B.spref[segoff + 2] = lenoff + sla + slb;
-      B.scode[segoff + 2] = (uint8_t)scc;
-    }
-    __syncwarp();
+  // the elements of the segments [0, nsegs) of B (spref: running element counts)
+  auto flush = [&](int nsegs_total, int total) {
     for (int t0 = 0; t0 < total; t0 += 32) {
       const int t = t0 + lane;
       bool keep = false;
@@ -387,6 +385,167 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
       count += __popc(bal);
     }
     __syncwarp();
+  };
+  // segments of one per lane (len 0: none) into B, then their elements
+  auto emit1 = [&](int32_t st0, int32_t len, int code) {
+    const bool has = len > 0;
+    const unsigned bal = __ballot_sync(FULL, has);
+    const int at = __popc(bal & lanemask_lt());
+    int tot;
+    const int off = warp_excl_scan(len, lane, &tot);
+    if (has) B.sstart[at] = st0, B.spref[at] = off, B.scode[at] = (uint8_t)code;
+    __syncwarp();
+    if (bal) flush(__popc(bal), tot);
+  };
+  // the sub-grid rows of dense cell (cx, cy, cz), image (mx, my, mz), that the ball reaches
+  auto dense_cell = [&](int cx, int cy, int cz, int mx, int my, int mz, int code) {
+    const int64_t cc = (int64_t)cx + (int64_t)J.G[0] * (cy + (int64_t)J.G[1] * cz);
+    const int f = __ldg(J.cell_f + cc);
+    const int64_t fb = __ldg(J.cell_fbase + cc);
+    const int c3[3] = {cx, cy, cz}, m3[3] = {mx, my, mz};
+    int fl[3], fh[3], fa[3];
+    double clo[3], chi[3], hf[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      fa[i] = i < J.dim ? f : 1;
+      clo[i] = cell_lo(i, c3[i], m3[i]);
+      chi[i] = cell_hi(i, c3[i], m3[i]);
+      hf[i] = J.gh[i] / fa[i];
+      fl[i] = 0, fh[i] = fa[i] - 1;
+      if (!all) {
+        const double base = J.ga[i] + c3[i] * J.gh[i] + m3[i] * J.gw[i];
+        const double a = floor((xa[i] - R - base) / hf[i]) - 1.0, b = floor((xa[i] + R - base) / hf[i]) + 1.0;
+        fl[i] = a < 0.0 ? 0 : (a > fa[i] - 1 ? fa[i] - 1 : (int)a);
+        fh[i] = b > fa[i] - 1 ? fa[i] - 1 : (b < 0.0 ? 0 : (int)b);
+      }
+    }
+    auto fine_d = [&](int i, int fi) -> double {
+      const double base = J.ga[i] + c3[i] * J.gh[i] + m3[i] * J.gw[i];
+      const double blo = fi == 0 ? clo[i] : base + fi * hf[i] - J.geps[i];
+      const double bhi = fi == fa[i] - 1 ? chi[i] : base + (fi + 1) * hf[i] + J.geps[i];
+      return dist1(i, blo, bhi);
+    };
+    const int fny = fh[1] - fl[1] + 1, fnz = fh[2] - fl[2] + 1;
+    const int nr = fny * fnz;
+    for (int r0 = 0; r0 < nr; r0 += 32) {
+      const int r = r0 + lane;
+      int32_t st0 = 0, len = 0;
+      if (r < nr) {
+        const int fy = fl[1] + r % fny, fz = fl[2] + r / fny;
+        const double dy = fine_d(1, fy), dz = fine_d(2, fz);
+        const double byz2 = dy * dy + dz * dz;
+        if (all || byz2 < R2v) {
+          int first = 1 << 30, last = -1;
+          for (int fx = fl[0]; fx <= fh[0]; fx++) {
+            const double dx = fine_d(0, fx);
+            if (all || dx * dx + byz2 < R2v) {
+              first = min(first, fx);
+              last = max(last, fx);
+            }
+          }
+          if (last >= first) {
+            const int64_t row = fb + (int64_t)fa[0] * (fy + (int64_t)fa[1] * fz);
+            st0 = __ldg(J.fine_abs + row + first);
+            len = __ldg(J.fine_abs + row + last + 1) - st0;
+          }
+        }
+      }
+      emit1(st0, len, code);
+    }
+  };
+
+  for (int row0 = 0; row0 < nrows; row0 += 32) {
+    const int row = row0 + lane;
+    int nseg = 0;
+    int32_t s0a = 0, s0b = 0, s0c = 0, sla = 0, slb = 0, slc = 0;
+    int sca = 0, scb = 0, scc = 0;
+    // cell ranges holding a dense cell, deferred (one per image): c0 | c1 << 16, 0: none
+    int dfr[3] = {-1, -1, -1};
+    int my = 0, mz = 0, cy = 0, cz = 0;
+    if (row < nrows) {
+      const int uy = lo[1] + row % ny, uz = lo[2] + row / ny;
+      const double dy = box_d(1, uy), dz = box_d(2, uz);
+      const double byz2 = dy * dy + dz * dz;
+      if (all || byz2 < R2v) {
+        int first = 1 << 30, last = -(1 << 30);
+        for (int ux = lo[0]; ux <= hi[0]; ux++) {
+          double dx = box_d(0, ux);
+          if (all || dx * dx + byz2 < R2v) {
+            first = min(first, ux);
+            last = max(last, ux);
+          }
+        }
+        const int Gx = J.G[0], Gy = J.G[1], Gz = J.G[2];
+        my = uy < 0 ? -1 : (uy >= Gy ? 1 : 0);
+        mz = uz < 0 ? -1 : (uz >= Gz ? 1 : 0);
+        cy = uy - my * Gy, cz = uz - mz * Gz;
+        const int64_t rowbase = (int64_t)Gx * (cy + (int64_t)Gy * cz);
+        for (int mx = -1; mx <= 1; mx++) {
+          int a = max(first, mx * Gx), b = min(last, mx * Gx + Gx - 1);
+          if (a > b) continue;
+          int c0 = a - mx * Gx, c1 = b - mx * Gx;
+          if (J.dprefix != nullptr &&
+              __ldg(J.dprefix + rowbase + c1 + 1) > __ldg(J.dprefix + rowbase + c0)) {
+            dfr[mx + 1] = c0 | (c1 << 16);
+            continue;
+          }
+          int32_t ps = __ldg(J.cell_start + rowbase + c0);
+          int32_t pe = __ldg(J.cell_start + rowbase + c1 + 1);
+          if (pe > ps) {
+            const int code = (mx + 1) + 3 * (my + 1) + 9 * (mz + 1);
+            if (nseg == 0) {
+              s0a = ps, sla = pe - ps, sca = code;
+            } else if (nseg == 1) {
+              s0b = ps, slb = pe - ps, scb = code;
+            } else {
+              s0c = ps, slc = pe - ps, scc = code;
+            }
+            nseg++;
+          }
+        }
+      }
+    }
+    int nsegs_total;
+    const int segoff = warp_excl_scan(nseg, lane, &nsegs_total);
+    const int mylen = sla + slb + slc;
+    int total;
+    const int lenoff = warp_excl_scan(mylen, lane, &total);
+    if (nseg > 0) {
+      B.sstart[segoff] = s0a, B.spref[segoff] = lenoff, B.scode[segoff] = (uint8_t)sca;
+    }
+    if (nseg > 1) {
+      B.sstart[segoff + 1] = s0b, B.spref[segoff + 1] = lenoff + sla;
+      B.scode[segoff + 1] = (uint8_t)scb;
+    }
+    if (nseg > 2) {
+      B.sstart[segoff + 2] = s0c, B.spref[segoff + 2] = lenoff + sla + slb;
+      B.scode[segoff + 2] = (uint8_t)scc;
+    }
+    __syncwarp();
+    flush(nsegs_total, total);
+    // the deferred ranges, cell by cell (a sparse cell is one segment)
+    for (int im = 0; im < 3; im++) {
+      unsigned pend = __ballot_sync(FULL, dfr[im] >= 0);
+      while (pend) {
+        const int src = __ffs(pend) - 1;
+        pend &= pend - 1;
+        const int rg = __shfl_sync(FULL, dfr[im], src);
+        const int ry = __shfl_sync(FULL, cy, src), rz = __shfl_sync(FULL, cz, src);
+        const int rmy = __shfl_sync(FULL, my, src), rmz = __shfl_sync(FULL, mz, src);
+        const int mx = im - 1;
+        const int code = (mx + 1) + 3 * (rmy + 1) + 9 * (rmz + 1);
+        const int64_t rowbase = (int64_t)J.G[0] * (ry + (int64_t)J.G[1] * rz);
+        for (int c = rg & 0xffff; c <= (rg >> 16); c++) {
+          if (__ldg(J.cell_f + rowbase + c) > 0) {
+            dense_cell(c, ry, rz, mx, rmy, rmz, code);
+          } else {
+            const int32_t ps = __ldg(J.cell_start + rowbase + c);
+            const int32_t pe = __ldg(J.cell_start + rowbase + c + 1);
+            emit1(ps, lane == 0 ? pe - ps : 0, code);
+          }
+        }
+      }
+    }
   }
   *exhausted = all && !__any_sync(FULL, beyond > 0);
   return count;

@@ -209,7 +209,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
 
   // ---- ConvexCell::build neighbour loop (convex_cell.rs:316-356) ----
-  double R = J.R0;
+  double R = first_radius(J, x);
   double lo2 = 0.0;
   long long processed = 0;
   bool finished = false;
@@ -219,10 +219,12 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     bool all;
     int cnt = gather_shell<T::CMAX>(J, S.u.g.sh, lane, x, R, lo2, ext, &all);
     int shrink = 0;
-    while (cnt > T::CMAX && shrink < 8) {
-      // too many candidates for the shell buffer: pull the outer radius in
+    while (cnt > T::CMAX && shrink < 48) {
+      // too many candidates for the shell buffer: pull the outer radius in, by the
+      // factor that would leave about half the buffer at uniform density
       const double rin = sqrt(lo2);
-      R = rin + 0.5 * (R - rin);
+      const double f = fmin(fmax(cbrt(0.5 * T::CMAX / (double)cnt), 0.1), 0.7);
+      R = rin + f * (R - rin);
       cnt = gather_shell<T::CMAX>(J, S.u.g.sh, lane, x, R, lo2, ext, &all);
       shrink++;
     }

@@ -5,6 +5,7 @@
 // generators into a row-major uniform grid (SoA positions, coalesced for the shell
 // gather of the cell kernel), and the serial flatten + Voronoi::finalize
 // (voronoi.rs:226, 241-263) with scans and scatters.
+#include <algorithm>
 #include <cstdint>
 
 #include "mv_internal.h"
@@ -63,6 +64,7 @@ __global__ void ext_finish_kernel(const unsigned long long* ext_keys, double* ex
 struct GridParams {
   int G[3];
   double a[3], inv[3];
+  int dim;
 };
 
 __global__ void cell_index_kernel(const double* __restrict__ gen, int n, GridParams gp,
@@ -89,6 +91,103 @@ __global__ void scatter_kernel(const double* __restrict__ gen, int n, const int3
   if (k >= n) return;
   int c = cid[k];
   int pos = start[c] + atomicAdd(fill + c, 1);
+  sx[pos] = gen[3 * (int64_t)k];
+  sy[pos] = gen[3 * (int64_t)k + 1];
+  sz[pos] = gen[3 * (int64_t)k + 2];
+  sid[pos] = k;
+}
+
+// --------------------------------------------------- dense cells (2nd level) --
+// A coarse cell holding more than DENSE_MIN generators gets a sub-grid of f cells along
+// each active axis (f = ceil((count / 2)^(1/dim)), f^dim <= 2^18; one cell along the
+// extruded axes): its generators are stored sorted by sub-cell, row-major (x fastest),
+// so that a query scans only the sub-cells its ball reaches.  cell_f[c] = f (0: no
+// sub-grid), cell_fbase[c] = first slot of the cell's f^dim + 1 entries in fine_abs
+// (absolute sorted positions; the last entry is the cell's end).
+constexpr int DENSE_MIN = 32;
+
+__device__ __forceinline__ int ipow(int f, int d) { return d == 1 ? f : (d == 2 ? f * f : f * f * f); }
+
+__global__ void dense_flag_kernel(const int32_t* __restrict__ count, int64_t ncell, int dim,
+                                  int32_t* __restrict__ dflag, int32_t* __restrict__ cell_f,
+                                  int32_t* __restrict__ fsize) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int m = count[c];
+  int f = 0;
+  if (m > DENSE_MIN) {
+    const int fmax = dim == 3 ? 64 : (dim == 2 ? 512 : 262144);
+    f = (int)ceil(pow(0.5 * (double)m, 1.0 / dim));
+    f = f < 2 ? 2 : (f > fmax ? fmax : f);
+  }
+  dflag[c] = f > 0;
+  cell_f[c] = f;
+  fsize[c] = f > 0 ? ipow(f, dim) + 1 : 0;
+}
+
+// sub-cell of generator k in its coarse cell (the coarse index is cell_index_kernel's)
+__device__ __forceinline__ int fine_index(const double* g, GridParams gp, int cid, int f) {
+  const int cx = cid % gp.G[0], cy = (cid / gp.G[0]) % gp.G[1], cz = cid / (gp.G[0] * gp.G[1]);
+  const int cc[3] = {cx, cy, cz};
+  int fi[3], fa[3];
+  for (int i = 0; i < 3; i++) {
+    fa[i] = i < gp.dim ? f : 1;
+    double t = floor(((g[i] - gp.a[i]) * gp.inv[i] - (double)cc[i]) * (double)fa[i]);
+    if (!(t >= 0.0)) t = 0.0;
+    if (t > fa[i] - 1) t = fa[i] - 1;
+    fi[i] = (int)t;
+  }
+  return fi[0] + fa[0] * (fi[1] + fa[1] * fi[2]);
+}
+
+__global__ void fine_count_kernel(const double* __restrict__ gen, int n, GridParams gp,
+                                  const int32_t* __restrict__ cid, const int32_t* __restrict__ cell_f,
+                                  const int64_t* __restrict__ cell_fbase, int32_t* __restrict__ fid,
+                                  int32_t* __restrict__ fine_cnt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = cid[k];
+  const int f = cell_f[c];
+  if (f == 0) return;
+  const int q = fine_index(gen + 3 * (int64_t)k, gp, c, f);
+  fid[k] = q;
+  atomicAdd(fine_cnt + cell_fbase[c] + q, 1);
+}
+
+// fine_abs[j] = start of the coarse cell + (fine_pos[j] - fine_pos[first slot of the cell])
+__global__ void fine_abs_kernel(const int32_t* __restrict__ start, const int32_t* __restrict__ cell_f,
+                                const int64_t* __restrict__ cell_fbase, int64_t ncell, int dim,
+                                const int32_t* __restrict__ fine_pos, int32_t* __restrict__ fine_abs) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncell; c += warps) {
+    const int f = cell_f[c];
+    if (f == 0) continue;
+    const int64_t b = cell_fbase[c];
+    const int32_t s0 = start[c], p0 = fine_pos[b];
+    const int slots = ipow(f, dim) + 1;
+    for (int j = lane; j < slots; j += 32) fine_abs[b + j] = s0 + (fine_pos[b + j] - p0);
+  }
+}
+
+__global__ void scatter_dense_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ cid,
+                                     const int32_t* __restrict__ start, int32_t* __restrict__ fill,
+                                     const int32_t* __restrict__ cell_f,
+                                     const int64_t* __restrict__ cell_fbase,
+                                     const int32_t* __restrict__ fid, const int32_t* __restrict__ fine_abs,
+                                     int32_t* __restrict__ fine_fill, double* __restrict__ sx,
+                                     double* __restrict__ sy, double* __restrict__ sz,
+                                     int32_t* __restrict__ sid) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = cid[k];
+  int pos;
+  if (cell_f[c] > 0) {
+    const int64_t j = cell_fbase[c] + fid[k];
+    pos = fine_abs[j] + atomicAdd(fine_fill + j, 1);
+  } else {
+    pos = start[c] + atomicAdd(fill + c, 1);
+  }
   sx[pos] = gen[3 * (int64_t)k];
   sy[pos] = gen[3 * (int64_t)k + 1];
   sz[pos] = gen[3 * (int64_t)k + 2];
@@ -285,9 +384,53 @@ void launch_grid(const double* gen, int n, const int G[3], const double a[3], co
                  double* sz, int32_t* sid, long long* scan_tmp, cudaStream_t st) {
   GridParams gp;
   for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
+  gp.dim = 3;
   int64_t ncell = (int64_t)G[0] * G[1] * G[2];
   if (n > 0) cell_index_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, count);
   scan_i32_to_i32(count, ncell, start, scan_tmp, st);
+  if (n > 0) scatter_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, cid, start, fill, sx, sy, sz, sid);
+}
+
+// First half of the two-level grid: coarse cell index, counts, starts and the dense
+// cells (flags, running count, sub-grid sizes).  The host reads the number of dense
+// cells and of fine slots, then calls launch_grid_fine (or scatters coarse-only).
+void launch_grid_coarse(const double* gen, int n, const int G[3], const double a[3],
+                        const double inv[3], int32_t* cid, int32_t* count, int32_t* start,
+                        int32_t* dflag, int32_t* dprefix, int32_t* cell_f, int32_t* fsize,
+                        int64_t* cell_fbase, int dim, long long* scan_tmp, cudaStream_t st) {
+  GridParams gp;
+  for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
+  gp.dim = dim;
+  const int64_t ncell = (int64_t)G[0] * G[1] * G[2];
+  if (n > 0) cell_index_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, count);
+  scan_i32_to_i32(count, ncell, start, scan_tmp, st);
+  dense_flag_kernel<<<nblk(ncell, 256), 256, 0, st>>>(count, ncell, dim, dflag, cell_f, fsize);
+  scan_i32_to_i32(dflag, ncell, dprefix, scan_tmp, st);
+  scan_i32_to_i64(fsize, ncell, cell_fbase, scan_tmp, st);
+}
+
+void launch_grid_fine(const double* gen, int n, const int G[3], const double a[3],
+                      const double inv[3], const int32_t* cid, const int32_t* start, int32_t* fill,
+                      const int32_t* cell_f, const int64_t* cell_fbase, int64_t nfine, int32_t* fid,
+                      int32_t* fine_cnt, int32_t* fine_pos, int32_t* fine_abs, double* sx, double* sy,
+                      double* sz, int32_t* sid, int dim, long long* scan_tmp, cudaStream_t st) {
+  GridParams gp;
+  for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
+  gp.dim = dim;
+  const int64_t ncell = (int64_t)G[0] * G[1] * G[2];
+  cudaMemsetAsync(fine_cnt, 0, 4 * (size_t)nfine, st);
+  if (n > 0) fine_count_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, cell_f, cell_fbase, fid, fine_cnt);
+  scan_i32_to_i32(fine_cnt, nfine, fine_pos, scan_tmp, st);
+  fine_abs_kernel<<<(int)std::min<int64_t>((ncell + 7) / 8, 65535 * 8), 256, 0, st>>>(
+      start, cell_f, cell_fbase, ncell, dim, fine_pos, fine_abs);
+  cudaMemsetAsync(fine_cnt, 0, 4 * (size_t)nfine, st);  // reused as the fill counters
+  if (n > 0)
+    scatter_dense_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, cid, start, fill, cell_f, cell_fbase,
+                                                      fid, fine_abs, fine_cnt, sx, sy, sz, sid);
+}
+
+void launch_scatter(const double* gen, int n, const int32_t* cid, const int32_t* start,
+                    int32_t* fill, double* sx, double* sy, double* sz, int32_t* sid, cudaStream_t st) {
   if (n > 0) scatter_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, cid, start, fill, sx, sy, sz, sid);
 }
 

@@ -71,6 +71,13 @@ struct Job {
   const double* ext;        // device [6]: min x,y,z, max x,y,z of the generators
   double geps[3];           // cell-box inflation against rounding of the cell index
   double R0;                // first neighbour-shell radius
+  // second grid level in dense cells (all nullptr when no cell is dense): generators of
+  // a dense cell are sorted by sub-cell (row-major, f^3 sub-cells)
+  const int32_t* dprefix;   // [ncell + 1] number of dense cells before each cell (row-major)
+  const int32_t* cell_f;    // [ncell] sub-grid resolution f, 0: not dense
+  const int64_t* cell_fbase;  // [ncell] first slot of the cell in fine_abs
+  const int32_t* fine_abs;  // sub-cell -> first sorted position ([fbase + f^3] = cell end)
+  double ppc_mean;          // generators per grid cell on average (first-radius scaling)
   // periodic image of shift code c = (mx+1) + 3(my+1) + 9(mz+1): the reference's query
   // offset s = (-m) w (rtree_nn.rs:86) and emitted shift -s (rtree_nn.rs:27-33)
   double qshift[27][3];
@@ -121,6 +128,7 @@ struct StageJob {
   int32_t cstride;            // candidate-list entries per cell
   uint32_t* cand;             // [nitems][cstride]: sorted position * 27 + shift code
   int32_t* info;              // [nitems]: count | exhausted << 30, 0: inactive, -1: retry
+  double* rad;                // [nitems]: radius of the first shell (first_radius)
   int64_t* rec_off;           // [nitems]: word offset of the cell record, -1: none
   double* rec;                // cell records (planes, vertices) for the integral kernel
   int64_t rec_cap;            // record words available to the chunk

@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     }
     const D3 x = load_gen(J, self);
     bool all = false;
-    const int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, J.R0, 0.0, ext_s, &all);
+    const double R = first_radius(J, x);
+    const int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all);
     if (cnt > SHELL_CMAX || cnt == 0) {
       if (lane == 0) SJ.info[item] = -1;
       continue;
@@ -107,7 +108,10 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
       self_first = sort_and_write<4>(B, lane, cnt, self, out);
     // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
     // fused kernel reports the error otherwise
-    if (lane == 0) SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
+    if (lane == 0) {
+      SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
+      SJ.rad[item] = R;
+    }
     __syncwarp();
   }
 }
@@ -433,7 +437,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   }
   // the list ends: the shell was complete up to the initial radius (as the fused
   // kernel's shell loop decides); otherwise the fused kernel continues the stream
-  if (!finished && !(exhausted || sr < J.R0 * (1.0 - 1e-12))) return CELL_RETRY;
+  if (!finished && !(exhausted || sr < SJ.rad[item] * (1.0 - 1e-12))) return CELL_RETRY;
 
   // ---- the cell record for the integral kernel ----
   if (!write_record(J, SJ.rec, SJ.rec_cap, SJ.rec_counter, SJ.rec_off + item, S, lane, x, np, nv, sr))

@@ -61,3 +61,26 @@ def poisson(n, seed=3, periodic=True, dim=3):
 def poisson_256(seed=3):
     """256^3 = 16,777,216 i.i.d. uniform points in [0,1)^3, periodic (the headline)."""
     return poisson(256 ** 3, seed=seed, periodic=True)
+
+
+def clustered(n=8388608, nclumps=2000, seed=4, periodic=True, dim=3):
+    """Clustered, uneven density: half of the n points i.i.d. uniform in [0,1)^dim, half
+    drawn from nclumps isotropic Gaussian clumps with centres uniform in the box, sigma
+    log-uniform in [1e-4, 1e-2] and Pareto(alpha = 1.5) weights normalised to the clump
+    counts (multinomial); clump points are wrapped into the unit box.  With the defaults
+    the local density spans about four orders of magnitude."""
+    rng = np.random.default_rng(seed)
+    nb = n // 2
+    pts = [rng.uniform(0.0, 1.0, size=(nb, 3))]
+    centres = rng.uniform(0.0, 1.0, size=(nclumps, 3))
+    sigma = np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), size=nclumps))
+    w = rng.pareto(1.5, size=nclumps) + 1.0
+    counts = rng.multinomial(n - nb, w / w.sum())
+    for c, s, k in zip(centres, sigma, counts):
+        if k:
+            pts.append(np.mod(c + s * rng.standard_normal((k, 3)), 1.0))
+    g = np.concatenate(pts)
+    if dim < 3:
+        g[:, dim:] = 0.0
+    return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=dim,
+                periodic=periodic, name=f"clustered_{n}_{nclumps}clumps_{'periodic' if periodic else 'rect'}")

@@ -26,6 +26,9 @@ def _case(name):
     if name == "lattice6_periodic":
         return dict(g=W.perturbed_grid([0, 0, 0], [1, 1, 1], 6, 0.0, None), a=[0, 0, 0],
                     w=[1, 1, 1], dim=3, per=True)
+    if name == "clustered8k_periodic":
+        return dict(g=W.clustered(8000, 20, seed=21)["generators"], a=[0, 0, 0], w=[1, 1, 1],
+                    dim=3, per=True)
     if name == "plane20_periodic_2d":
         return dict(g=W.perturbed_plane([0, 0, 0], [1, 1, 1], 20, 0.9, rng), a=[0, 0, 0],
                     w=[1, 1, 1], dim=2, per=True)
@@ -61,7 +64,7 @@ def _compare(ca, ex, faces):
 @pytest.mark.parametrize("pipeline", ["fused", "staged"])
 @pytest.mark.parametrize("faces", [False, True])
 @pytest.mark.parametrize("name", ["poisson3k_periodic", "grid12_w2", "lattice6_periodic",
-                                  "plane20_periodic_2d"])
+                                  "plane20_periodic_2d", "clustered8k_periodic"])
 def test_cells_export_parity(gpu_ctx, oracle, name, faces, pipeline):
     c = _case(name)
     if faces and c["dim"] != 3:

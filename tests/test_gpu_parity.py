@@ -60,6 +60,15 @@ def _case(name):
     if name == "non_perturbed_z":
         fx = json.load(open(os.path.join(HERE, "golden", "non_perturbed_z.json")))
         return dict(generators=fx["generators"], anchor=fx["anchor"], width=fx["width"], dim=3, periodic=False)
+    if name == "clustered30k_periodic":
+        return dict(generators=W.clustered(30000, 60, seed=11)["generators"], anchor=[0, 0, 0],
+                    width=[1, 1, 1], dim=3, periodic=True)
+    if name == "clustered20k_rect":
+        return dict(generators=W.clustered(20000, 40, seed=12)["generators"], anchor=[0, 0, 0],
+                    width=[1, 1, 1], dim=3, periodic=False)
+    if name == "clustered_2d_periodic":
+        return dict(generators=W.clustered(12000, 30, seed=13, dim=2)["generators"],
+                    anchor=[0, 0, 0], width=[1, 1, 1], dim=2, periodic=True)
     if name == "degenerate_2e15":
         g = W.perturbed_grid([0, 0, 0], [2e15] * 3, 10, 0.0, None)
         g[42] = 1e14 * np.array([1.00007490802, 9.00019014286, 5.00014639879])
@@ -70,7 +79,8 @@ def _case(name):
 CASES = ["single", "two", "five_2d", "four_2d_periodic", "lattice4_rect", "lattice12_periodic",
          "jitter16_rect", "grid15_w2", "poisson20k_periodic", "poisson5k_rect_aniso",
          "small_periodic_17", "plane25_periodic_2d", "poisson_2d_rect", "line_1d_periodic",
-         "non_perturbed_z", "degenerate_2e15"]
+         "non_perturbed_z", "degenerate_2e15", "clustered30k_periodic", "clustered20k_rect",
+         "clustered_2d_periodic"]
 
 
 def _rel_err(a, b, scale):
