@@ -7,7 +7,7 @@ ordering and the cell -> face CSR.  Default workload: 256^3 = 16,777,216 i.i.d.
 uniform generators in the periodic unit box (seeded, synthetic).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision filtered|fp64]
-                  [--workload poisson_256|lattice_64|jitter_32] [--impl ours|reference]
+                  [--workload poisson_256|lattice_64|jitter_32|clustered] [--impl ours|reference]
                   [--pipeline auto|staged|fused]
 
 The default pipeline runs the staged shell / clip / integral kernels; the plain FP64
@@ -73,6 +73,10 @@ def workload(name: str, seed: int):
         w = W.exact_lattice(64)
     elif name == "jitter_32":
         w = W.jittered_lattice_32(seed)
+    elif name == "clustered":
+        w = W.clustered(8388608, 2000, seed=seed)
+    elif name.startswith("clustered_"):
+        w = W.clustered(int(name.split("_")[1]), 2000, seed=seed)
     elif name.startswith("poisson_"):
         n = int(name.split("_")[1]) ** 3
         w = W.poisson(n, seed=seed, periodic=True)

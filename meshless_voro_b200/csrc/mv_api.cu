@@ -21,6 +21,7 @@
 namespace mv {
 // mv_cells.cu
 cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
+size_t cells_big_bytes(int blocks_fast, int blocks_large);
 int cells_blocks_per_sm_fast(int precision);
 int cells_blocks_per_sm_large(int precision);
 // mv_export.cu
@@ -44,13 +45,13 @@ void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long l
                  double* ext, int* bad, cudaStream_t st);
 void launch_grid_coarse(const double* gen, int n, const int G[3], const double a[3],
                         const double inv[3], int32_t* cid, int32_t* count, int32_t* start,
-                        int32_t* dflag, int32_t* dprefix, int32_t* cell_f, int32_t* fsize,
-                        int64_t* cell_fbase, int dim, long long* scan_tmp, cudaStream_t st);
-void launch_grid_fine(const double* gen, int n, const int G[3], const double a[3],
-                      const double inv[3], const int32_t* cid, const int32_t* start, int32_t* fill,
-                      const int32_t* cell_f, const int64_t* cell_fbase, int64_t nfine, int32_t* fid,
-                      int32_t* fine_cnt, int32_t* fine_pos, int32_t* fine_abs, double* sx, double* sy,
-                      double* sz, int32_t* sid, int dim, long long* scan_tmp, cudaStream_t st);
+                        int32_t* dflag, int32_t* dprefix, int dim, long long* scan_tmp, cudaStream_t st);
+size_t grid_dense_sort_bytes(int n, int64_t ncell);
+cudaError_t launch_grid_dense(const double* gen, int n, const int G[3], const double a[3],
+                              const double inv[3], int dim, const int32_t* cid, const int32_t* dflag,
+                              unsigned long long* key_a, unsigned long long* key_b, int32_t* val_a,
+                              int32_t* val_b, void* sort_tmp, size_t sort_bytes, double* sx,
+                              double* sy, double* sz, int32_t* sid, uint32_t* fkey, cudaStream_t st);
 void launch_scatter(const double* gen, int n, const int32_t* cid, const int32_t* start,
                     int32_t* fill, double* sx, double* sy, double* sz, int32_t* sid, cudaStream_t st);
 size_t scan_tmp_elems(int64_t n);
@@ -159,12 +160,13 @@ struct Workspace {
   DevBuf in_xyz, in_mask;
   DevBuf gen, sx, sy, sz, sid, cid;
   DevBuf cell_count, cell_start, cell_fill, scan_tmp;
-  DevBuf dflag, dprefix, cell_f, fsize, cell_fbase, fid, fine_cnt, fine_pos, fine_abs;
+  DevBuf dflag, dprefix, dkey_a, dkey_b, dval_a, dval_b, dsort_tmp, fkey;
   DevBuf volume, centroid, sr, face_count, stage_off, face_off;
   DevBuf in_count, conn_count, conn_off, cursor, conn;
   DevBuf st_left, st_right, st_area, st_cen, st_nrm, st_code;
   DevBuf f_left, f_right, f_area, f_cen, f_nrm, f_code;
   DevBuf ovf_a, ovf_b;
+  DevBuf big;  // staging slots of the fused kernel for large shells
   DevBuf counters;
   // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
   DevBuf cand, cand_info, cand_rad, rec_off, rec, retry, stage_ctr;
@@ -467,10 +469,6 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   e |= ensure(ctx, W.cell_fill, 4 * (ncell + 1));
   e |= ensure(ctx, W.dflag, 4 * (ncell + 1));
   e |= ensure(ctx, W.dprefix, 4 * (ncell + 1));
-  e |= ensure(ctx, W.cell_f, 4 * (ncell + 1));
-  e |= ensure(ctx, W.fsize, 4 * (ncell + 1));
-  e |= ensure(ctx, W.cell_fbase, 8 * (ncell + 1));
-  e |= ensure(ctx, W.fid, 4 * N);
   e |= ensure(ctx, W.scan_tmp, 8 * (scan_tmp_elems(std::max<int64_t>(ncell + 1, N)) + 64));
   e |= ensure(ctx, W.volume, 8 * N);
   e |= ensure(ctx, W.centroid, 24 * N);
@@ -519,27 +517,28 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     launch_prep(d_xyz, ni, s.dim, P<double>(W.gen), C->ext_keys, C->ext, &C->bad_input, st);
     launch_grid_coarse(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
                        P<int32_t>(W.cell_count), P<int32_t>(W.cell_start), P<int32_t>(W.dflag),
-                       P<int32_t>(W.dprefix), P<int32_t>(W.cell_f), P<int32_t>(W.fsize),
-                       P<int64_t>(W.cell_fbase), s.dim, P<long long>(W.scan_tmp), st);
+                       P<int32_t>(W.dprefix), s.dim, P<long long>(W.scan_tmp), st);
     int32_t ndense = 0;
-    int64_t nfine = 0;
     MV_CUDA(cudaMemcpyAsync(&ndense, P<int32_t>(W.dprefix) + ncell, 4, cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaMemcpyAsync(&nfine, P<int64_t>(W.cell_fbase) + ncell, 8, cudaMemcpyDeviceToHost, st));
     MV_CUDA(cudaStreamSynchronize(st));
     if (ndense > 0) {
-      // clustered input: the dense cells get a second grid level
+      // clustered input: the dense cells are ordered by Morton key (a radix sort)
+      const size_t sort_bytes = grid_dense_sort_bytes(ni, ncell);
       e = 0;
-      e |= ensure(ctx, W.fine_cnt, 4 * (size_t)nfine);
-      e |= ensure(ctx, W.fine_pos, 4 * (size_t)(nfine + 1));
-      e |= ensure(ctx, W.fine_abs, 4 * (size_t)nfine);
+      e |= ensure(ctx, W.dkey_a, 8 * N);
+      e |= ensure(ctx, W.dkey_b, 8 * N);
+      e |= ensure(ctx, W.dval_a, 4 * N);
+      e |= ensure(ctx, W.dval_b, 4 * N);
+      e |= ensure(ctx, W.fkey, 4 * N);
+      e |= ensure(ctx, W.dsort_tmp, sort_bytes + 256);
       if (e) return MV_ERR_OOM;
-      launch_grid_fine(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, P<int32_t>(W.cid),
-                       P<int32_t>(W.cell_start), P<int32_t>(W.cell_fill), P<int32_t>(W.cell_f),
-                       P<int64_t>(W.cell_fbase), nfine, P<int32_t>(W.fid), P<int32_t>(W.fine_cnt),
-                       P<int32_t>(W.fine_pos), P<int32_t>(W.fine_abs), P<double>(W.sx),
-                       P<double>(W.sy), P<double>(W.sz), P<int32_t>(W.sid), s.dim,
-                       P<long long>(W.scan_tmp), st);
-      launches += 6;
+      MV_CUDA(launch_grid_dense(P<double>(W.gen), ni, s.G, s.anchor, s.ginv, s.dim, P<int32_t>(W.cid),
+                                P<int32_t>(W.dflag), P<unsigned long long>(W.dkey_a),
+                                P<unsigned long long>(W.dkey_b), P<int32_t>(W.dval_a),
+                                P<int32_t>(W.dval_b), W.dsort_tmp.p, W.dsort_tmp.cap, P<double>(W.sx),
+                                P<double>(W.sy), P<double>(W.sz), P<int32_t>(W.sid),
+                                P<uint32_t>(W.fkey), st));
+      launches += 6;  // keys, gather and the sort's passes
     } else {
       launch_scatter(P<double>(W.gen), ni, P<int32_t>(W.cid), P<int32_t>(W.cell_start),
                      P<int32_t>(W.cell_fill), P<double>(W.sx), P<double>(W.sy), P<double>(W.sz),
@@ -557,9 +556,8 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.cell_start = P<int32_t>(W.cell_start);
     if (ndense > 0) {
       J.dprefix = P<int32_t>(W.dprefix);
-      J.cell_f = P<int32_t>(W.cell_f);
-      J.cell_fbase = P<int64_t>(W.cell_fbase);
-      J.fine_abs = P<int32_t>(W.fine_abs);
+      J.cell_dense = P<int32_t>(W.dflag);
+      J.fkey = P<uint32_t>(W.fkey);
     }
     J.mask = d_mask;
     J.n = ni;
@@ -579,6 +577,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     J.ext = C->ext;
     J.R0 = s.R0;
+    J.fbits = fkey_bits(s.dim);
     J.ppc_mean = (double)std::max<int64_t>(n, 1) / (double)ncell;
     for (int c = 0; c < 27; c++) {
       const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
@@ -613,6 +612,12 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.status = C->status;
     J.stats = C->stats;
     const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
+    {
+      const size_t bb = cells_big_bytes(ctx->sm_count * std::max(1, ctx->bps_fast[pi]),
+                                        ctx->sm_count * std::max(1, ctx->bps_large[pi]));
+      if (ensure(ctx, W.big, bb)) return MV_ERR_OOM;
+      J.big = static_cast<char*>(W.big.p);
+    }
     const bool staged = use_staged(o, n);
     if (exporting) {
       // every built cell leaves a record: the staged clip kernel and the fused kernel

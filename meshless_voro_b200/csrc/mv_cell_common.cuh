@@ -231,43 +231,56 @@ struct CellCount {
 #define WCNT(CC, slot, v) ((CC).c[slot] += (unsigned)(v))
 
 // ------------------------------------------------------------- neighbour shell --
-// Radius of a cell's first shell: R0, scaled down in dense cells by the local density
-// (of the generator's sub-cell when it holds a few generators, else of its grid cell)
-// so that the first shell holds about as many candidates as in a uniform region.
-// Shells are prefixes of the same nearest-first stream, so the radius only moves work
-// between shells, never the result.
-__device__ __forceinline__ double first_radius(const Job& J, D3 x) {
-  if (J.cell_f == nullptr) return J.R0;
+// First position in [a, b) whose dense-cell key is >= k (the keys of a dense cell are
+// sorted).
+__device__ __forceinline__ int32_t fkey_lower_bound(const Job& J, int32_t a, int32_t b, uint32_t k) {
+  while (a < b) {
+    const int32_t m = (a + b) >> 1;
+    if (__ldg(J.fkey + m) < k)
+      a = m + 1;
+    else
+      b = m;
+  }
+  return a;
+}
+
+// Radius of a cell's first shell: R0, scaled down in dense cells by the local density,
+// taken from the finest octree cell around the generator that still holds 8 generators
+// (lane l counts level l), so that the first shell holds about as many candidates as in
+// a uniform region.  Shells are prefixes of the same nearest-first stream, so the
+// radius only moves work between shells, never the result.
+__device__ __forceinline__ double first_radius(const Job& J, D3 x, int lane) {
+  if (J.fkey == nullptr) return J.R0;
   const double xa[3] = {x.x, x.y, x.z};
   int c[3];
-  double t[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    t[i] = (xa[i] - J.ga[i]) * J.ginv[i];
-    double f = floor(t[i]);
+    double f = floor((xa[i] - J.ga[i]) * J.ginv[i]);
     if (!(f >= 0.0)) f = 0.0;
     if (f > J.G[i] - 1) f = J.G[i] - 1;
     c[i] = (int)f;
   }
   const int64_t cc = (int64_t)c[0] + (int64_t)J.G[0] * (c[1] + (int64_t)J.G[1] * c[2]);
-  const int f = __ldg(J.cell_f + cc);
-  if (f == 0) return J.R0;
-  const int cnt = __ldg(J.cell_start + cc + 1) - __ldg(J.cell_start + cc);
-  int q[3], fa[3];
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    fa[i] = i < J.dim ? f : 1;
-    double u = floor((t[i] - (double)c[i]) * (double)fa[i]);
-    if (!(u >= 0.0)) u = 0.0;
-    if (u > fa[i] - 1) u = fa[i] - 1;
-    q[i] = (int)u;
+  if (!__ldg(J.cell_dense + cc)) return J.R0;
+  const int32_t cs = __ldg(J.cell_start + cc), ce = __ldg(J.cell_start + cc + 1);
+  const int B = J.fbits, dim = J.dim;
+  uint32_t q[3] = {0u, 0u, 0u};
+  for (int i = 0; i < dim; i++) q[i] = fine_q(xa[i], J.ga[i], J.ginv[i], c[i], B);
+  const uint32_t key = morton(dim, q[0], q[1], q[2]);
+  int cl = 0;
+  if (lane <= B) {
+    const int sh = dim * (B - lane);
+    const uint32_t klo = (key >> sh) << sh;
+    const int32_t a = fkey_lower_bound(J, cs, ce, klo);
+    cl = fkey_lower_bound(J, a, ce, klo + (1u << sh)) - a;
   }
-  const int64_t slot = __ldg(J.cell_fbase + cc) + q[0] + (int64_t)fa[0] * (q[1] + (int64_t)fa[1] * q[2]);
-  const int cf = __ldg(J.fine_abs + slot + 1) - __ldg(J.fine_abs + slot);
-  const double nsub = (double)fa[0] * fa[1] * fa[2];
-  const double ratio = cf >= 4 ? (double)cf * nsub / J.ppc_mean : (double)cnt / J.ppc_mean;
+  const unsigned bal = __ballot_sync(FULL, lane <= B && cl >= 8);
+  if (bal == 0u) return J.R0;
+  const int L = 31 - __clz(bal);
+  const int cnt = __shfl_sync(FULL, cl, L);
+  const double ratio = (double)cnt * exp2((double)(dim * L)) / J.ppc_mean;
   if (!(ratio > 1.0)) return J.R0;
-  return J.R0 * pow(ratio, -1.0 / J.dim);
+  return J.R0 * pow(ratio, -1.0 / dim);
 }
 
 template <int CMAX>
@@ -277,11 +290,143 @@ struct ShellBuf {
   int32_t cpos[CMAX];            // grid-sorted position of the generator
   int32_t sstart[96];
   int32_t spref[97];
+  int32_t gbin;                  // next bin of a staged shell (big shells), -1: none
   uint8_t scode[96];
 };
 
+// ------------------------------------------------------------------ big shells --
+// A shell of the fused kernel that holds more than the shared-memory buffer (up to
+// BIG_CAP elements) is staged in the warp's slot of a global buffer, bucketed by d2 into
+// BIG_BINS bins and consumed group by group, each group (whole bins, at most CMAX
+// elements) sorted in shared memory.  Bins are monotone in d2, so the groups come in
+// stream order and each group sorted by (d2, tie) continues the nearest-first stream
+// exactly.  Dense clumps make such shells common: the safety radius of a cell on the
+// surface of a compact clump takes in the whole clump.
+constexpr int BIG_CAP = 4096;
+constexpr int BIG_BINS = 256;
+constexpr size_t BIG_SLOT_BYTES = (size_t)BIG_CAP * 32 + BIG_BINS * 4;
+
+struct BigView {
+  unsigned long long* keyA;  // the gathered shell (elements >= CMAX; the rest in shared)
+  unsigned long long* keyB;  // the shell bucketed by bin
+  uint32_t* tieA;
+  uint32_t* tieB;
+  int32_t* cposA;
+  int32_t* cposB;
+  int32_t* pinc;             // [BIG_BINS] inclusive prefix of the bin counts
+};
+
+__device__ __forceinline__ BigView big_view(char* slot) {
+  BigView V;
+  V.keyA = reinterpret_cast<unsigned long long*>(slot);
+  V.keyB = V.keyA + BIG_CAP;
+  V.tieA = reinterpret_cast<uint32_t*>(V.keyB + BIG_CAP);
+  V.tieB = V.tieA + BIG_CAP;
+  V.cposA = reinterpret_cast<int32_t*>(V.tieB + BIG_CAP);
+  V.cposB = V.cposA + BIG_CAP;
+  V.pinc = V.cposB + BIG_CAP;
+  return V;
+}
+
+__device__ __forceinline__ int big_bin(unsigned long long key, double lo2, double scale) {
+  const double t = (__longlong_as_double((long long)key) - lo2) * scale;
+  return t >= (double)(BIG_BINS - 1) ? BIG_BINS - 1 : (t > 0.0 ? (int)t : 0);
+}
+
+// Buckets the cnt (CMAX < cnt <= BIG_CAP) elements of a gathered shell [lo2, R2) into
+// the slot's B arrays by bin and returns the largest bin count; when that exceeds CMAX
+// nothing is bucketed and the caller narrows the shell instead.
+template <int CMAX>
+__device__ __noinline__ int big_bucket(ShellBuf<CMAX>& B, char* slot, int lane, int cnt, double lo2,
+                                       double R2) {
+  static_assert(CMAX * 8 >= BIG_BINS * 4, "bin counters live in the key array");
+  const BigView V = big_view(slot);
+  for (int i = lane; i < CMAX; i += 32) {
+    V.keyA[i] = B.key[i];
+    V.tieA[i] = B.tie[i];
+    V.cposA[i] = B.cpos[i];
+  }
+  __syncwarp();
+  int* H = reinterpret_cast<int*>(B.key);
+  for (int i = lane; i < BIG_BINS; i += 32) H[i] = 0;
+  __syncwarp();
+  const double scale = (double)BIG_BINS / (R2 - lo2);
+  for (int i = lane; i < cnt; i += 32) atomicAdd(&H[big_bin(V.keyA[i], lo2, scale)], 1);
+  __syncwarp();
+  constexpr int PER = BIG_BINS / 32;
+  int c[PER];
+  int sum = 0, mx = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    c[k] = H[PER * lane + k];
+    sum += c[k];
+    mx = max(mx, c[k]);
+  }
+  mx = (int)__reduce_max_sync(FULL, (unsigned)mx);
+  if (mx > CMAX) return mx;
+  int tot;
+  int ex = warp_excl_scan(sum, lane, &tot);
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    H[PER * lane + k] = ex;
+    ex += c[k];
+    V.pinc[PER * lane + k] = ex;
+  }
+  __syncwarp();
+  for (int i = lane; i < cnt; i += 32) {
+    const unsigned long long key = V.keyA[i];
+    const int pos = atomicAdd(&H[big_bin(key, lo2, scale)], 1);
+    V.keyB[pos] = key;
+    V.tieB[pos] = V.tieA[i];
+    V.cposB[pos] = V.cposA[i];
+  }
+  __syncwarp();
+  return mx;
+}
+
+// Loads the next group of whole bins, starting at bin B.gbin, that holds at most CMAX
+// elements into B (unsorted) and returns its size; B.gbin moves past the group (-1
+// after the last bin).
+template <int CMAX>
+__device__ __noinline__ int big_group(ShellBuf<CMAX>& B, char* slot, int lane) {
+  const BigView V = big_view(slot);
+  const int b = B.gbin;
+  const int base = b > 0 ? V.pinc[b - 1] : 0;
+  constexpr int PER = BIG_BINS / 32;
+  int nb = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const int kk = PER * lane + k;
+    nb += (kk >= b && V.pinc[kk] <= base + CMAX) ? 1 : 0;
+  }
+  nb = (int)__reduce_add_sync(FULL, (unsigned)nb);
+  const int end = V.pinc[b + nb - 1];
+  for (int i = lane; i < end - base; i += 32) {
+    B.key[i] = V.keyB[base + i];
+    B.tie[i] = V.tieB[base + i];
+    B.cpos[i] = V.cposB[base + i];
+  }
+  if (lane == 0) B.gbin = b + nb < BIG_BINS ? b + nb : -1;
+  __syncwarp();
+  return end - base;
+}
+
+// The warp's staging slot (global warp index) and the count at which a gather stops.
+__device__ __forceinline__ char* big_slot(const Job& J) {
+  if (J.big == nullptr) return nullptr;
+  const size_t w = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  return J.big + w * BIG_SLOT_BYTES;
+}
+template <int CMAX>
+__device__ __forceinline__ int big_stop(const Job& J) {
+  return J.big != nullptr ? BIG_CAP : 32 * CMAX;
+}
+
 // Gathers every stream element (generator, periodic image) with lo2 <= d2 < R*R into
-// B (unsorted) and returns how many there are (may exceed CMAX).  *exhausted is set
+// B (unsorted) and returns how many there are (may exceed CMAX; once the count passes
+// stop the gather ends early and returns a count above stop).  With BIG and a slot,
+// elements CMAX .. BIG_CAP - 1 go to the slot's A arrays.  *exhausted is set
 // when the enumerated cells cover every image and none lies beyond R, i.e. the stream
 // ends with this shell.  d2 is the reference's squared distance:
 // (g - q).length_squared() for nn_iter (rstar) and |(q + s) - g|^2 for
@@ -290,11 +435,12 @@ struct ShellBuf {
 // Grid rows (y, z) go to lanes; a lane turns the cells of its row that the ball
 // reaches into contiguous segments of sorted positions (one per periodic image).  A
 // segment that contains a dense cell (J.dprefix) is deferred: its cells are then
-// visited one by one, and a dense cell contributes the rows of its sub-grid that the
-// ball reaches.  Without the ball test (all images enumerated) every sub-cell counts.
-template <int CMAX>
+// visited one by one, and a dense cell contributes the octree cells that the shell
+// reaches.  Without the ball test (all images enumerated) every cell counts whole.
+template <int CMAX, bool BIG = false>
 __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
-                                         double lo2, const double* ext, bool* exhausted) {
+                                         double lo2, const double* ext, bool* exhausted,
+                                         int stop, char* big = nullptr) {
   const double xa[3] = {x.x, x.y, x.z};
   int lo[3], hi[3];
   bool all = true;
@@ -343,7 +489,7 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
 
   // the elements of the segments [0, nsegs) of B (spref: running element counts)
   auto flush = [&](int nsegs_total, int total) {
-    for (int t0 = 0; t0 < total; t0 += 32) {
+    for (int t0 = 0; t0 < total && count <= stop; t0 += 32) {
       const int t = t0 + lane;
       bool keep = false;
       double d2 = 0.0;
@@ -381,6 +527,11 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
         B.key[pos] = (unsigned long long)__double_as_longlong(d2);
         B.tie[pos] = tie;
         B.cpos[pos] = s;
+      } else if (BIG && keep && big != nullptr && pos < BIG_CAP) {
+        const BigView V = big_view(big);
+        V.keyA[pos] = (unsigned long long)__double_as_longlong(d2);
+        V.tieA[pos] = tie;
+        V.cposA[pos] = s;
       }
       count += __popc(bal);
     }
@@ -397,64 +548,72 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
     __syncwarp();
     if (bal) flush(__popc(bal), tot);
   };
-  // the sub-grid rows of dense cell (cx, cy, cz), image (mx, my, mz), that the ball reaches
+  // the octree cells of dense cell (cx, cy, cz), image (mx, my, mz), that the shell
+  // [lo, R) reaches, at the level whose cells are at least R / 2 wide (at most five per
+  // axis); a cell that lies inside the inner radius holds no element of the shell
   auto dense_cell = [&](int cx, int cy, int cz, int mx, int my, int mz, int code) {
     const int64_t cc = (int64_t)cx + (int64_t)J.G[0] * (cy + (int64_t)J.G[1] * cz);
-    const int f = __ldg(J.cell_f + cc);
-    const int64_t fb = __ldg(J.cell_fbase + cc);
+    const int32_t cs = __ldg(J.cell_start + cc), ce = __ldg(J.cell_start + cc + 1);
+    if (all) {
+      emit1(cs, lane == 0 ? ce - cs : 0, code);
+      return;
+    }
+    const int B = J.fbits, dim = J.dim;
+    double hmin = J.gh[0];
+    for (int i = 1; i < dim; i++) hmin = fmin(hmin, J.gh[i]);
+    const double r = 2.0 * hmin / R;
+    const int L = r >= 2.0 ? min(B, ilogb(r)) : 0;
+    const int nL = 1 << L;
     const int c3[3] = {cx, cy, cz}, m3[3] = {mx, my, mz};
-    int fl[3], fh[3], fa[3];
-    double clo[3], chi[3], hf[3];
+    int ja[3], jn[3];
+    double base[3], w[3], clo[3], chi[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      fa[i] = i < J.dim ? f : 1;
       clo[i] = cell_lo(i, c3[i], m3[i]);
       chi[i] = cell_hi(i, c3[i], m3[i]);
-      hf[i] = J.gh[i] / fa[i];
-      fl[i] = 0, fh[i] = fa[i] - 1;
-      if (!all) {
-        const double base = J.ga[i] + c3[i] * J.gh[i] + m3[i] * J.gw[i];
-        const double a = floor((xa[i] - R - base) / hf[i]) - 1.0, b = floor((xa[i] + R - base) / hf[i]) + 1.0;
-        fl[i] = a < 0.0 ? 0 : (a > fa[i] - 1 ? fa[i] - 1 : (int)a);
-        fh[i] = b > fa[i] - 1 ? fa[i] - 1 : (b < 0.0 ? 0 : (int)b);
+      base[i] = J.ga[i] + c3[i] * J.gh[i] + m3[i] * J.gw[i];
+      w[i] = J.gh[i] / nL;
+      ja[i] = 0, jn[i] = 1;
+      if (i < dim) {
+        const double fa = floor((xa[i] - R - base[i] - J.geps[i]) / w[i]);
+        const double fb = floor((xa[i] + R - base[i] + J.geps[i]) / w[i]);
+        const int lo_j = fa < 0.0 ? 0 : (fa > nL - 1 ? nL - 1 : (int)fa);
+        const int hi_j = fb > nL - 1 ? nL - 1 : (fb < 0.0 ? 0 : (int)fb);
+        ja[i] = lo_j, jn[i] = hi_j - lo_j + 1;
       }
     }
-    auto fine_d = [&](int i, int fi) -> double {
-      const double base = J.ga[i] + c3[i] * J.gh[i] + m3[i] * J.gw[i];
-      const double blo = fi == 0 ? clo[i] : base + fi * hf[i] - J.geps[i];
-      const double bhi = fi == fa[i] - 1 ? chi[i] : base + (fi + 1) * hf[i] + J.geps[i];
-      return dist1(i, blo, bhi);
-    };
-    const int fny = fh[1] - fl[1] + 1, fnz = fh[2] - fl[2] + 1;
-    const int nr = fny * fnz;
-    for (int r0 = 0; r0 < nr; r0 += 32) {
-      const int r = r0 + lane;
+    const int sh = dim * (B - L);
+    const int ncl = jn[0] * jn[1] * jn[2];
+    const double lo2p = lo2 * (1.0 - 1e-9);
+    for (int r0 = 0; r0 < ncl && count <= stop; r0 += 32) {
+      const int t = r0 + lane;
       int32_t st0 = 0, len = 0;
-      if (r < nr) {
-        const int fy = fl[1] + r % fny, fz = fl[2] + r / fny;
-        const double dy = fine_d(1, fy), dz = fine_d(2, fz);
-        const double byz2 = dy * dy + dz * dz;
-        if (all || byz2 < R2v) {
-          int first = 1 << 30, last = -1;
-          for (int fx = fl[0]; fx <= fh[0]; fx++) {
-            const double dx = fine_d(0, fx);
-            if (all || dx * dx + byz2 < R2v) {
-              first = min(first, fx);
-              last = max(last, fx);
-            }
+      if (t < ncl) {
+        const int j[3] = {ja[0] + t % jn[0], ja[1] + (t / jn[0]) % jn[1], ja[2] + t / (jn[0] * jn[1])};
+        double dmin2 = 0.0, dmax2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double blo = clo[i], bhi = chi[i];
+          if (i < dim) {
+            if (j[i] > 0) blo = base[i] + j[i] * w[i] - J.geps[i];
+            if (j[i] < nL - 1) bhi = base[i] + (j[i] + 1) * w[i] + J.geps[i];
           }
-          if (last >= first) {
-            const int64_t row = fb + (int64_t)fa[0] * (fy + (int64_t)fa[1] * fz);
-            st0 = __ldg(J.fine_abs + row + first);
-            len = __ldg(J.fine_abs + row + last + 1) - st0;
-          }
+          const double dn = dist1(i, blo, bhi);
+          const double df = fmax(fabs(xa[i] - blo), fabs(bhi - xa[i]));
+          dmin2 += dn * dn;
+          dmax2 += df * df;
+        }
+        if (dmin2 < R2v && !(dmax2 < lo2p)) {
+          const uint32_t klo = morton(dim, (uint32_t)j[0], (uint32_t)j[1], (uint32_t)j[2]) << sh;
+          st0 = fkey_lower_bound(J, cs, ce, klo);
+          len = fkey_lower_bound(J, st0, ce, klo + (1u << sh)) - st0;
         }
       }
       emit1(st0, len, code);
     }
   };
 
-  for (int row0 = 0; row0 < nrows; row0 += 32) {
+  for (int row0 = 0; row0 < nrows && count <= stop; row0 += 32) {
     const int row = row0 + lane;
     int nseg = 0;
     int32_t s0a = 0, s0b = 0, s0c = 0, sla = 0, slb = 0, slc = 0;
@@ -535,8 +694,8 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
         const int mx = im - 1;
         const int code = (mx + 1) + 3 * (rmy + 1) + 9 * (rmz + 1);
         const int64_t rowbase = (int64_t)J.G[0] * (ry + (int64_t)J.G[1] * rz);
-        for (int c = rg & 0xffff; c <= (rg >> 16); c++) {
-          if (__ldg(J.cell_f + rowbase + c) > 0) {
+        for (int c = rg & 0xffff; c <= (rg >> 16) && count <= stop; c++) {
+          if (__ldg(J.cell_dense + rowbase + c)) {
             dense_cell(c, ry, rz, mx, rmy, rmz, code);
           } else {
             const int32_t ps = __ldg(J.cell_start + rowbase + c);
@@ -547,7 +706,7 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
       }
     }
   }
-  *exhausted = all && !__any_sync(FULL, beyond > 0);
+  *exhausted = all && count <= stop && !__any_sync(FULL, beyond > 0);
   return count;
 }
 

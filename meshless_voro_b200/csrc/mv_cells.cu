@@ -26,6 +26,7 @@
 // decision; neighbours certified to remove no vertex are consumed without building
 // their f64 bisector plane, and the first neighbour that needs attention gets the
 // reference's f64 (and, when undecided, exact integer) treatment.
+#include <algorithm>
 #include <cstdint>
 
 #include "mv_cell_common.cuh"
@@ -209,7 +210,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
 
   // ---- ConvexCell::build neighbour loop (convex_cell.rs:316-356) ----
-  double R = first_radius(J, x);
+  double R = first_radius(J, x, lane);
   double lo2 = 0.0;
   long long processed = 0;
   bool finished = false;
@@ -217,214 +218,233 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   for (int shell = 0; !finished; shell++) {
     if (shell > 0) WCNT(cc, ST_SHELLS, 1);
     bool all;
-    int cnt = gather_shell<T::CMAX>(J, S.u.g.sh, lane, x, R, lo2, ext, &all);
+    int cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, big_stop<T::CMAX>(J),
+                                          big_slot(J));
     int shrink = 0;
-    while (cnt > T::CMAX && shrink < 48) {
-      // too many candidates for the shell buffer: pull the outer radius in, by the
-      // factor that would leave about half the buffer at uniform density
-      const double rin = sqrt(lo2);
-      const double f = fmin(fmax(cbrt(0.5 * T::CMAX / (double)cnt), 0.1), 0.7);
-      R = rin + f * (R - rin);
-      cnt = gather_shell<T::CMAX>(J, S.u.g.sh, lane, x, R, lo2, ext, &all);
+    bool staged = false;
+    for (;;) {
+      if (cnt <= T::CMAX) break;
+      if (J.big != nullptr && cnt <= BIG_CAP &&
+          big_bucket<T::CMAX>(S.u.g.sh, big_slot(J), lane, cnt, lo2, R * R) <= T::CMAX) {
+        staged = true;
+        break;
+      }
+      if (shrink >= 48) break;
+      // too many candidates: pull the outer radius in, so that the shell keeps about
+      // half of what fits (by volume, at the density just seen)
+      const double rin3 = lo2 * sqrt(lo2);
+      const double fits = J.big != nullptr ? (double)BIG_CAP : (double)T::CMAX;
+      const double g = fmin(fmax(0.5 * fits / (double)cnt, 1e-3), 0.7);
+      R = cbrt(rin3 + (R * R * R - rin3) * g);
+      cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, big_stop<T::CMAX>(J),
+                                        big_slot(J));
       shrink++;
     }
-    if (cnt > T::CMAX) return CELL_OVERFLOW;
-    sort_shell<T::CMAX>(S.u.g.sh, lane, cnt);
-    int j = 0;
-    if (processed == 0 && cnt > 0) {
-      // the first neighbour must be the generator itself (convex_cell.rs:325-329)
-      if ((int)(S.u.g.sh.tie[0] / 27u) != self) {
-        *err_code = MV_ERR_DEGENERATE;
-        return CELL_ERROR;
-      }
-      j = 1;
-    }
-    while (j < cnt) {
-      const int kb = min(PREC == MV_PRECISION_FILTERED ? K : 1, cnt - j);
-      unsigned bad, stop;
-      setup_batch<T, PREC>(J, S, lane, j, kb, x, x1, sr, A, &bad, &stop);
-      const int fb = bad ? __ffs(bad) - 1 : kb, fs = stop ? __ffs(stop) - 1 : kb;
-      const int limit = min(fb, fs);
-      // first neighbour in [0, limit) that may remove a vertex
-      int kstar = limit;
-      for (int k = 0; k < limit; k++) {
-        bool need = !S.u.g.bfilt[k];
-        if (!need) {
-          const float ex = S.u.g.bex[k], ey = S.u.g.bey[k], ez = S.u.g.bez[k];
-          const float h = S.u.g.bh[k], Tk = S.u.g.bT[k];
-#pragma unroll
-          for (int w = 0; w < T::NW; w++) {
-            const int q = lane + 32 * w;
-            if (q < nv) {
-              const int sl = S.ord[q];
-              const float4 f = S.f4[sl];
-              const float s = fmaf(ez, f.z, fmaf(ey, f.y, fmaf(ex, f.x, h)));
-              need = need || !(fabsf(s) > Tk) || s < 0.f;
-            }
-          }
-        }
-        if (__any_sync(FULL, need)) {
-          kstar = k;
-          break;
-        }
-      }
-      WCNT(cc, ST_NEIGHBOURS, kstar);
-      if (kstar == limit) {
-        // neighbours [0, limit) remove nothing
-        j += limit;
-        if (limit < kb) {
-          if (fb <= fs) {
-            *err_code = MV_ERR_DEGENERATE;  // convex_cell.rs:342
-            return CELL_ERROR;
-          }
-          finished = true;  // safety radius reached (convex_cell.rs:343-345)
-          break;
-        }
-        K = min(2 * K, T::KMAX);
-        continue;
-      }
-      WCNT(cc, ST_NEIGHBOURS, 1);
-      // ---- neighbour kstar: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
-      const D3 dx = {S.u.g.bdx[kstar], S.u.g.bdy[kstar], S.u.g.bdz[kstar]};
-      const double dist = S.u.g.bdist[kstar];
-      const D3 ngb = {S.u.g.bgx[kstar], S.u.g.bgy[kstar], S.u.g.bgz[kstar]};
-      const int orig = S.u.g.borig[kstar];
-      const int code = S.u.g.bcode[kstar];
-      const bool filt = S.u.g.bfilt[kstar];
-      const float ex = S.u.g.bex[kstar], ey = S.u.g.bey[kstar], ez = S.u.g.bez[kstar];
-      const float h = S.u.g.bh[kstar], Tk = S.u.g.bT[kstar];
-      j += kstar + 1;
-      K = 1;
-      const D3 n = divs(dx, dist);
-      const D3 p = scale(0.5, add(x, ngb));
-      const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
-      const double d = dot(n, p);
-      unsigned rm[T::NW];
-      int n_und = 0, n_ex = 0;
-#pragma unroll
-      for (int w = 0; w < T::NW; w++) {
-        const int q = lane + 32 * w;
-        bool removed = false;
-        if (q < nv) {
-          const int sl = S.ord[q];
-          bool decided = false;
-          if (PREC == MV_PRECISION_FILTERED && filt) {
-            const float4 f = S.f4[sl];
-            const float s = fmaf(ez, f.z, fmaf(ey, f.y, fmaf(ex, f.x, h)));
-            if (fabsf(s) > Tk) {
-              removed = s < 0.f;
-              decided = true;
-            }
-          }
-          if (!decided) {
-            n_und++;
-            const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
-            if (fabs(c) < errb) {
-              removed = exact_clip(J, S, sl, x, ngb) < 0;
-              n_ex++;
-            } else {
-              removed = c < 0.0;
-            }
-          }
-        }
-        rm[w] = __ballot_sync(FULL, removed);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        n_und += __shfl_xor_sync(FULL, n_und, o);
-        n_ex += __shfl_xor_sync(FULL, n_ex, o);
-      }
-      if (PREC == MV_PRECISION_FILTERED) WCNT(cc, ST_F32_UNDECIDED, n_und);
-      WCNT(cc, ST_EXACT, n_ex);
-      int nrem = 0;
-#pragma unroll
-      for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
-      if (nrem == 0) continue;
-
-      // ---- a vertex was clipped: add the plane (convex_cell.rs:393-418) ----
-      if (np >= T::PMAX) return CELL_OVERFLOW;
-      const int p_idx = np;
-      if (lane == 0) {
-        S.pnx[p_idx] = n.x, S.pny[p_idx] = n.y, S.pnz[p_idx] = n.z;
-        S.ppx[p_idx] = p.x, S.ppy[p_idx] = p.y, S.ppz[p_idx] = p.z;
-        S.pd[p_idx] = d;
-        S.pright[p_idx] = orig;
-        S.pcode[p_idx] = (uint8_t)code;
-      }
-      np++;
-      WCNT(cc, ST_PLANES, 1);
-
-      // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
-      unsigned km[T::NW];
-      int totK = 0;
-#pragma unroll
-      for (int w = 0; w < T::NW; w++) {
-        km[w] = ~rm[w] & valid_bits(nv, w);
-        totK += __popc(km[w]);
-      }
-      const int nvf = totK;
-      {
-        int dest[T::NW];
-        PIdx held[T::NW];
-#pragma unroll
-        for (int w = 0; w < T::NW; w++) {
-          const int q = lane + 32 * w;
-          int dd = -1;
-          held[w] = 0;
-          if (q < nv) {
-            held[w] = S.ord[q];
-            if (!((rm[w] >> lane) & 1u)) {
-              dd = q < nvf ? q : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, q));
-            } else if (q <= nvf) {
-              const int t = rank_below<T::NW>(rm, q) + 1;
-              dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
-            } else {
-              dd = q - 1;
-            }
-          }
-          dest[w] = dd;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int w = 0; w < T::NW; w++)
-          if (dest[w] >= 0) S.ord[dest[w]] = held[w];
-        __syncwarp();
-      }
-
-      // ring of the removed region (compute_boundary + SimpleCycle iteration)
-      int E = ring_parallel<T>(S, lane, nvf, nv);
-      if (E < 0) {
-        WCNT(cc, ST_SERIAL_RING, 1);
-        int e2 = 0;
-        if (lane == 0) e2 = ring_serial<T>(S, nvf, nv, np);
-        E = __shfl_sync(FULL, e2, 0);
-        __syncwarp();
-        if (E == -2) return CELL_OVERFLOW;
-        if (E < 0) {
-          *err_code = MV_ERR_RING;
+    if (cnt > T::CMAX && !staged) return CELL_OVERFLOW;
+    // a staged shell is consumed in groups of bins (the cursor lives in shared memory)
+    if (lane == 0) S.u.g.sh.gbin = staged ? 0 : -1;
+    __syncwarp();
+    if (staged) cnt = big_group<T::CMAX>(S.u.g.sh, big_slot(J), lane);
+    for (;;) {
+      sort_shell<T::CMAX>(S.u.g.sh, lane, cnt);
+      int j = 0;
+      if (processed == 0 && cnt > 0) {
+        // the first neighbour must be the generator itself (convex_cell.rs:325-329)
+        if ((int)(S.u.g.sh.tie[0] / 27u) != self) {
+          *err_code = MV_ERR_DEGENERATE;
           return CELL_ERROR;
         }
+        j = 1;
       }
-      if (nvf + E > T::VMAX) return CELL_OVERFLOW;
-      bool ok = true;
-      double r2n = 0.0;
-      for (int e = lane; e < E; e += 32)
-        ok &= make_vertex<PIdx>(S, S.ord[nvf + e], S.ea[e], S.eb[e], p_idx, x, dim, &r2n);
-      if (__any_sync(FULL, !ok)) {
-        *err_code = MV_ERR_DET;
-        return CELL_ERROR;
+      while (j < cnt) {
+        const int kb = min(PREC == MV_PRECISION_FILTERED ? K : 1, cnt - j);
+        unsigned bad, stop;
+        setup_batch<T, PREC>(J, S, lane, j, kb, x, x1, sr, A, &bad, &stop);
+        const int fb = bad ? __ffs(bad) - 1 : kb, fs = stop ? __ffs(stop) - 1 : kb;
+        const int limit = min(fb, fs);
+        // first neighbour in [0, limit) that may remove a vertex
+        int kstar = limit;
+        for (int k = 0; k < limit; k++) {
+          bool need = !S.u.g.bfilt[k];
+          if (!need) {
+            const float ex = S.u.g.bex[k], ey = S.u.g.bey[k], ez = S.u.g.bez[k];
+            const float h = S.u.g.bh[k], Tk = S.u.g.bT[k];
+  #pragma unroll
+            for (int w = 0; w < T::NW; w++) {
+              const int q = lane + 32 * w;
+              if (q < nv) {
+                const int sl = S.ord[q];
+                const float4 f = S.f4[sl];
+                const float s = fmaf(ez, f.z, fmaf(ey, f.y, fmaf(ex, f.x, h)));
+                need = need || !(fabsf(s) > Tk) || s < 0.f;
+              }
+            }
+          }
+          if (__any_sync(FULL, need)) {
+            kstar = k;
+            break;
+          }
+        }
+        WCNT(cc, ST_NEIGHBOURS, kstar);
+        if (kstar == limit) {
+          // neighbours [0, limit) remove nothing
+          j += limit;
+          if (limit < kb) {
+            if (fb <= fs) {
+              *err_code = MV_ERR_DEGENERATE;  // convex_cell.rs:342
+              return CELL_ERROR;
+            }
+            finished = true;  // safety radius reached (convex_cell.rs:343-345)
+            break;
+          }
+          K = min(2 * K, T::KMAX);
+          continue;
+        }
+        WCNT(cc, ST_NEIGHBOURS, 1);
+        // ---- neighbour kstar: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
+        const D3 dx = {S.u.g.bdx[kstar], S.u.g.bdy[kstar], S.u.g.bdz[kstar]};
+        const double dist = S.u.g.bdist[kstar];
+        const D3 ngb = {S.u.g.bgx[kstar], S.u.g.bgy[kstar], S.u.g.bgz[kstar]};
+        const int orig = S.u.g.borig[kstar];
+        const int code = S.u.g.bcode[kstar];
+        const bool filt = S.u.g.bfilt[kstar];
+        const float ex = S.u.g.bex[kstar], ey = S.u.g.bey[kstar], ez = S.u.g.bez[kstar];
+        const float h = S.u.g.bh[kstar], Tk = S.u.g.bT[kstar];
+        j += kstar + 1;
+        K = 1;
+        const D3 n = divs(dx, dist);
+        const D3 p = scale(0.5, add(x, ngb));
+        const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
+        const double d = dot(n, p);
+        unsigned rm[T::NW];
+        int n_und = 0, n_ex = 0;
+  #pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          const int q = lane + 32 * w;
+          bool removed = false;
+          if (q < nv) {
+            const int sl = S.ord[q];
+            bool decided = false;
+            if (PREC == MV_PRECISION_FILTERED && filt) {
+              const float4 f = S.f4[sl];
+              const float s = fmaf(ez, f.z, fmaf(ey, f.y, fmaf(ex, f.x, h)));
+              if (fabsf(s) > Tk) {
+                removed = s < 0.f;
+                decided = true;
+              }
+            }
+            if (!decided) {
+              n_und++;
+              const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
+              if (fabs(c) < errb) {
+                removed = exact_clip(J, S, sl, x, ngb) < 0;
+                n_ex++;
+              } else {
+                removed = c < 0.0;
+              }
+            }
+          }
+          rm[w] = __ballot_sync(FULL, removed);
+        }
+  #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          n_und += __shfl_xor_sync(FULL, n_und, o);
+          n_ex += __shfl_xor_sync(FULL, n_ex, o);
+        }
+        if (PREC == MV_PRECISION_FILTERED) WCNT(cc, ST_F32_UNDECIDED, n_und);
+        WCNT(cc, ST_EXACT, n_ex);
+        int nrem = 0;
+  #pragma unroll
+        for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
+        if (nrem == 0) continue;
+
+        // ---- a vertex was clipped: add the plane (convex_cell.rs:393-418) ----
+        if (np >= T::PMAX) return CELL_OVERFLOW;
+        const int p_idx = np;
+        if (lane == 0) {
+          S.pnx[p_idx] = n.x, S.pny[p_idx] = n.y, S.pnz[p_idx] = n.z;
+          S.ppx[p_idx] = p.x, S.ppy[p_idx] = p.y, S.ppz[p_idx] = p.z;
+          S.pd[p_idx] = d;
+          S.pright[p_idx] = orig;
+          S.pcode[p_idx] = (uint8_t)code;
+        }
+        np++;
+        WCNT(cc, ST_PLANES, 1);
+
+        // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
+        unsigned km[T::NW];
+        int totK = 0;
+  #pragma unroll
+        for (int w = 0; w < T::NW; w++) {
+          km[w] = ~rm[w] & valid_bits(nv, w);
+          totK += __popc(km[w]);
+        }
+        const int nvf = totK;
+        {
+          int dest[T::NW];
+          PIdx held[T::NW];
+  #pragma unroll
+          for (int w = 0; w < T::NW; w++) {
+            const int q = lane + 32 * w;
+            int dd = -1;
+            held[w] = 0;
+            if (q < nv) {
+              held[w] = S.ord[q];
+              if (!((rm[w] >> lane) & 1u)) {
+                dd = q < nvf ? q : select_bit<T::NW>(rm, totK - rank_below<T::NW>(km, q));
+              } else if (q <= nvf) {
+                const int t = rank_below<T::NW>(rm, q) + 1;
+                dd = ((t == 1) ? nv : select_bit<T::NW>(km, totK - t + 2)) - 1;
+              } else {
+                dd = q - 1;
+              }
+            }
+            dest[w] = dd;
+          }
+          __syncwarp();
+  #pragma unroll
+          for (int w = 0; w < T::NW; w++)
+            if (dest[w] >= 0) S.ord[dest[w]] = held[w];
+          __syncwarp();
+        }
+
+        // ring of the removed region (compute_boundary + SimpleCycle iteration)
+        int E = ring_parallel<T>(S, lane, nvf, nv);
+        if (E < 0) {
+          WCNT(cc, ST_SERIAL_RING, 1);
+          int e2 = 0;
+          if (lane == 0) e2 = ring_serial<T>(S, nvf, nv, np);
+          E = __shfl_sync(FULL, e2, 0);
+          __syncwarp();
+          if (E == -2) return CELL_OVERFLOW;
+          if (E < 0) {
+            *err_code = MV_ERR_RING;
+            return CELL_ERROR;
+          }
+        }
+        if (nvf + E > T::VMAX) return CELL_OVERFLOW;
+        bool ok = true;
+        double r2n = 0.0;
+        for (int e = lane; e < E; e += 32)
+          ok &= make_vertex<PIdx>(S, S.ord[nvf + e], S.ea[e], S.eb[e], p_idx, x, dim, &r2n);
+        if (__any_sync(FULL, !ok)) {
+          *err_code = MV_ERR_DET;
+          return CELL_ERROR;
+        }
+        __syncwarp();
+        nv = nvf + E;
+        // update_safety_radius (convex_cell.rs:443-453)
+        double m = 0.0;
+        for (int q = lane; q < nv; q += 32) m = fmax(m, S.vr2[S.ord[q]]);
+        max_r2 = warp_max_nonneg(m);
+        sr = 2.0 * sqrt(max_r2);
+        A = amax_of(max_r2, dim);
       }
-      __syncwarp();
-      nv = nvf + E;
-      // update_safety_radius (convex_cell.rs:443-453)
-      double m = 0.0;
-      for (int q = lane; q < nv; q += 32) m = fmax(m, S.vr2[S.ord[q]]);
-      max_r2 = warp_max_nonneg(m);
-      sr = 2.0 * sqrt(max_r2);
-      A = amax_of(max_r2, dim);
+      processed += cnt;
+      if (finished || S.u.g.sh.gbin < 0) break;
+      cnt = big_group<T::CMAX>(S.u.g.sh, big_slot(J), lane);
     }
     if (finished) break;
-    processed += cnt;
     if (all) break;
     if (sr < R * (1.0 - 1e-12)) break;
     lo2 = R * R;
@@ -539,6 +559,13 @@ int cells_blocks_per_sm_large(int precision) {
   return precision == MV_PRECISION_FILTERED
              ? blocks_per_sm<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>()
              : blocks_per_sm<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>();
+}
+
+// Bytes of the staging slots (one per warp) of fast-tier and large-tier grids of the
+// given sizes; the tiers run one after the other, so they share the slots.
+size_t cells_big_bytes(int blocks_fast, int blocks_large) {
+  const size_t warps = std::max((size_t)blocks_fast * FAST_WARPS, (size_t)blocks_large * LARGE_WARPS);
+  return warps * BIG_SLOT_BYTES;
 }
 
 cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st) {

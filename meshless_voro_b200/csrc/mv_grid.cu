@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <cstdint>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "mv_internal.h"
 
 namespace mv {
@@ -98,100 +100,55 @@ __global__ void scatter_kernel(const double* __restrict__ gen, int n, const int3
 }
 
 // --------------------------------------------------- dense cells (2nd level) --
-// A coarse cell holding more than DENSE_MIN generators gets a sub-grid of f cells along
-// each active axis (f = ceil((count / 2)^(1/dim)), f^dim <= 2^18; one cell along the
-// extruded axes): its generators are stored sorted by sub-cell, row-major (x fastest),
-// so that a query scans only the sub-cells its ball reaches.  cell_f[c] = f (0: no
-// sub-grid), cell_fbase[c] = first slot of the cell's f^dim + 1 entries in fine_abs
-// (absolute sorted positions; the last entry is the cell's end).
+// A coarse cell holding more than DENSE_MIN generators is dense: its generators are
+// stored sorted by the Morton key of their position inside the cell (fkey_bits(dim) bits
+// per active axis).  The cells of every level of the cell's implicit octree are then
+// contiguous ranges of sorted positions, found by binary search on the keys, so a
+// query scans the cells of the level that matches its radius, whatever the local
+// density (Gaussian clumps span many orders of magnitude inside one coarse cell).
+// Sparse cells keep key 0 and their generators in input order.
 constexpr int DENSE_MIN = 32;
 
-__device__ __forceinline__ int ipow(int f, int d) { return d == 1 ? f : (d == 2 ? f * f : f * f * f); }
-
-__global__ void dense_flag_kernel(const int32_t* __restrict__ count, int64_t ncell, int dim,
-                                  int32_t* __restrict__ dflag, int32_t* __restrict__ cell_f,
-                                  int32_t* __restrict__ fsize) {
+__global__ void dense_flag_kernel(const int32_t* __restrict__ count, int64_t ncell,
+                                  int32_t* __restrict__ dflag) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
-  const int m = count[c];
-  int f = 0;
-  if (m > DENSE_MIN) {
-    const int fmax = dim == 3 ? 64 : (dim == 2 ? 512 : 262144);
-    f = (int)ceil(pow(0.5 * (double)m, 1.0 / dim));
-    f = f < 2 ? 2 : (f > fmax ? fmax : f);
-  }
-  dflag[c] = f > 0;
-  cell_f[c] = f;
-  fsize[c] = f > 0 ? ipow(f, dim) + 1 : 0;
+  dflag[c] = count[c] > DENSE_MIN;
 }
 
-// sub-cell of generator k in its coarse cell (the coarse index is cell_index_kernel's)
-__device__ __forceinline__ int fine_index(const double* g, GridParams gp, int cid, int f) {
-  const int cx = cid % gp.G[0], cy = (cid / gp.G[0]) % gp.G[1], cz = cid / (gp.G[0] * gp.G[1]);
-  const int cc[3] = {cx, cy, cz};
-  int fi[3], fa[3];
-  for (int i = 0; i < 3; i++) {
-    fa[i] = i < gp.dim ? f : 1;
-    double t = floor(((g[i] - gp.a[i]) * gp.inv[i] - (double)cc[i]) * (double)fa[i]);
-    if (!(t >= 0.0)) t = 0.0;
-    if (t > fa[i] - 1) t = fa[i] - 1;
-    fi[i] = (int)t;
-  }
-  return fi[0] + fa[0] * (fi[1] + fa[1] * fi[2]);
-}
-
-__global__ void fine_count_kernel(const double* __restrict__ gen, int n, GridParams gp,
-                                  const int32_t* __restrict__ cid, const int32_t* __restrict__ cell_f,
-                                  const int64_t* __restrict__ cell_fbase, int32_t* __restrict__ fid,
-                                  int32_t* __restrict__ fine_cnt) {
+// sort key of generator k: coarse cell << FKEY_BITS | Morton key inside a dense cell
+__global__ void dense_key_kernel(const double* __restrict__ gen, int n, GridParams gp,
+                                 const int32_t* __restrict__ cid, const int32_t* __restrict__ dflag,
+                                 unsigned long long* __restrict__ key, int32_t* __restrict__ val) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int c = cid[k];
-  const int f = cell_f[c];
-  if (f == 0) return;
-  const int q = fine_index(gen + 3 * (int64_t)k, gp, c, f);
-  fid[k] = q;
-  atomicAdd(fine_cnt + cell_fbase[c] + q, 1);
+  uint32_t m = 0;
+  if (dflag[c]) {
+    const int bits = fkey_bits(gp.dim);
+    const int cc[3] = {c % gp.G[0], (c / gp.G[0]) % gp.G[1], c / (gp.G[0] * gp.G[1])};
+    uint32_t q[3] = {0u, 0u, 0u};
+    for (int i = 0; i < gp.dim; i++) q[i] = fine_q(gen[3 * (int64_t)k + i], gp.a[i], gp.inv[i], cc[i], bits);
+    m = morton(gp.dim, q[0], q[1], q[2]);
+  }
+  key[k] = ((unsigned long long)c << FKEY_BITS) | m;
+  val[k] = k;
 }
 
-// fine_abs[j] = start of the coarse cell + (fine_pos[j] - fine_pos[first slot of the cell])
-__global__ void fine_abs_kernel(const int32_t* __restrict__ start, const int32_t* __restrict__ cell_f,
-                                const int64_t* __restrict__ cell_fbase, int64_t ncell, int dim,
-                                const int32_t* __restrict__ fine_pos, int32_t* __restrict__ fine_abs) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncell; c += warps) {
-    const int f = cell_f[c];
-    if (f == 0) continue;
-    const int64_t b = cell_fbase[c];
-    const int32_t s0 = start[c], p0 = fine_pos[b];
-    const int slots = ipow(f, dim) + 1;
-    for (int j = lane; j < slots; j += 32) fine_abs[b + j] = s0 + (fine_pos[b + j] - p0);
-  }
-}
-
-__global__ void scatter_dense_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ cid,
-                                     const int32_t* __restrict__ start, int32_t* __restrict__ fill,
-                                     const int32_t* __restrict__ cell_f,
-                                     const int64_t* __restrict__ cell_fbase,
-                                     const int32_t* __restrict__ fid, const int32_t* __restrict__ fine_abs,
-                                     int32_t* __restrict__ fine_fill, double* __restrict__ sx,
-                                     double* __restrict__ sy, double* __restrict__ sz,
-                                     int32_t* __restrict__ sid) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const int c = cid[k];
-  int pos;
-  if (cell_f[c] > 0) {
-    const int64_t j = cell_fbase[c] + fid[k];
-    pos = fine_abs[j] + atomicAdd(fine_fill + j, 1);
-  } else {
-    pos = start[c] + atomicAdd(fill + c, 1);
-  }
-  sx[pos] = gen[3 * (int64_t)k];
-  sy[pos] = gen[3 * (int64_t)k + 1];
-  sz[pos] = gen[3 * (int64_t)k + 2];
-  sid[pos] = k;
+// sorted position s <- generator val[s]; fkey = the Morton part of its sort key
+__global__ void dense_gather_kernel(const double* __restrict__ gen, int n,
+                                    const unsigned long long* __restrict__ key,
+                                    const int32_t* __restrict__ val, double* __restrict__ sx,
+                                    double* __restrict__ sy, double* __restrict__ sz,
+                                    int32_t* __restrict__ sid, uint32_t* __restrict__ fkey) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int k = val[s];
+  sx[s] = gen[3 * (int64_t)k];
+  sy[s] = gen[3 * (int64_t)k + 1];
+  sz[s] = gen[3 * (int64_t)k + 2];
+  sid[s] = k;
+  fkey[s] = (uint32_t)(key[s] & ((1ull << FKEY_BITS) - 1ull));
 }
 
 // ------------------------------------------------------------------- scans --
@@ -392,41 +349,52 @@ void launch_grid(const double* gen, int n, const int G[3], const double a[3], co
 }
 
 // First half of the two-level grid: coarse cell index, counts, starts and the dense
-// cells (flags, running count, sub-grid sizes).  The host reads the number of dense
-// cells and of fine slots, then calls launch_grid_fine (or scatters coarse-only).
+// cells (flags and their running count).  The host reads the number of dense cells,
+// then calls launch_grid_dense (or scatters coarse-only).
 void launch_grid_coarse(const double* gen, int n, const int G[3], const double a[3],
                         const double inv[3], int32_t* cid, int32_t* count, int32_t* start,
-                        int32_t* dflag, int32_t* dprefix, int32_t* cell_f, int32_t* fsize,
-                        int64_t* cell_fbase, int dim, long long* scan_tmp, cudaStream_t st) {
+                        int32_t* dflag, int32_t* dprefix, int dim, long long* scan_tmp, cudaStream_t st) {
   GridParams gp;
   for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
   gp.dim = dim;
   const int64_t ncell = (int64_t)G[0] * G[1] * G[2];
   if (n > 0) cell_index_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, count);
   scan_i32_to_i32(count, ncell, start, scan_tmp, st);
-  dense_flag_kernel<<<nblk(ncell, 256), 256, 0, st>>>(count, ncell, dim, dflag, cell_f, fsize);
+  dense_flag_kernel<<<nblk(ncell, 256), 256, 0, st>>>(count, ncell, dflag);
   scan_i32_to_i32(dflag, ncell, dprefix, scan_tmp, st);
-  scan_i32_to_i64(fsize, ncell, cell_fbase, scan_tmp, st);
 }
 
-void launch_grid_fine(const double* gen, int n, const int G[3], const double a[3],
-                      const double inv[3], const int32_t* cid, const int32_t* start, int32_t* fill,
-                      const int32_t* cell_f, const int64_t* cell_fbase, int64_t nfine, int32_t* fid,
-                      int32_t* fine_cnt, int32_t* fine_pos, int32_t* fine_abs, double* sx, double* sy,
-                      double* sz, int32_t* sid, int dim, long long* scan_tmp, cudaStream_t st) {
+// Scratch bytes of launch_grid_dense's radix sort.
+size_t grid_dense_sort_bytes(int n, int64_t ncell) {
+  size_t bytes = 0;
+  int end_bit = FKEY_BITS;
+  while ((1ll << (end_bit - FKEY_BITS)) < ncell) end_bit++;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr,
+                                  (unsigned long long*)nullptr, (const int32_t*)nullptr,
+                                  (int32_t*)nullptr, n, 0, end_bit);
+  return bytes;
+}
+
+// Second half when some cells are dense: one stable radix sort of (cell, Morton key)
+// pairs orders the generators by coarse cell and, inside dense cells, by key.
+cudaError_t launch_grid_dense(const double* gen, int n, const int G[3], const double a[3],
+                              const double inv[3], int dim, const int32_t* cid, const int32_t* dflag,
+                              unsigned long long* key_a, unsigned long long* key_b, int32_t* val_a,
+                              int32_t* val_b, void* sort_tmp, size_t sort_bytes, double* sx,
+                              double* sy, double* sz, int32_t* sid, uint32_t* fkey, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
   GridParams gp;
   for (int i = 0; i < 3; i++) gp.G[i] = G[i], gp.a[i] = a[i], gp.inv[i] = inv[i];
   gp.dim = dim;
   const int64_t ncell = (int64_t)G[0] * G[1] * G[2];
-  cudaMemsetAsync(fine_cnt, 0, 4 * (size_t)nfine, st);
-  if (n > 0) fine_count_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, cell_f, cell_fbase, fid, fine_cnt);
-  scan_i32_to_i32(fine_cnt, nfine, fine_pos, scan_tmp, st);
-  fine_abs_kernel<<<(int)std::min<int64_t>((ncell + 7) / 8, 65535 * 8), 256, 0, st>>>(
-      start, cell_f, cell_fbase, ncell, dim, fine_pos, fine_abs);
-  cudaMemsetAsync(fine_cnt, 0, 4 * (size_t)nfine, st);  // reused as the fill counters
-  if (n > 0)
-    scatter_dense_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, cid, start, fill, cell_f, cell_fbase,
-                                                      fid, fine_abs, fine_cnt, sx, sy, sz, sid);
+  int end_bit = FKEY_BITS;
+  while ((1ll << (end_bit - FKEY_BITS)) < ncell) end_bit++;
+  dense_key_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, gp, cid, dflag, key_a, val_a);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, key_a, key_b, val_a, val_b,
+                                                  n, 0, end_bit, st);
+  if (e != cudaSuccess) return e;
+  dense_gather_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, key_b, val_b, sx, sy, sz, sid, fkey);
+  return cudaGetLastError();
 }
 
 void launch_scatter(const double* gen, int n, const int32_t* cid, const int32_t* start,

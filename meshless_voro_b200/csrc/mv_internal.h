@@ -1,5 +1,6 @@
 // mv_internal.h -- structures shared by the kernels and the host orchestration.
 #pragma once
+#include <cmath>
 #include <cstdint>
 
 namespace mv {
@@ -71,12 +72,14 @@ struct Job {
   const double* ext;        // device [6]: min x,y,z, max x,y,z of the generators
   double geps[3];           // cell-box inflation against rounding of the cell index
   double R0;                // first neighbour-shell radius
-  // second grid level in dense cells (all nullptr when no cell is dense): generators of
-  // a dense cell are sorted by sub-cell (row-major, f^3 sub-cells)
+  // second level in dense cells (all nullptr when no cell is dense): the generators of a
+  // dense cell are sorted by the Morton key of their position inside the cell (fbits
+  // bits per active axis, x lowest), so that every cell of the cell's implicit octree,
+  // at any level 0..fbits, is a contiguous range of sorted positions
   const int32_t* dprefix;   // [ncell + 1] number of dense cells before each cell (row-major)
-  const int32_t* cell_f;    // [ncell] sub-grid resolution f, 0: not dense
-  const int64_t* cell_fbase;  // [ncell] first slot of the cell in fine_abs
-  const int32_t* fine_abs;  // sub-cell -> first sorted position ([fbase + f^3] = cell end)
+  const int32_t* cell_dense;  // [ncell] 1: dense
+  const uint32_t* fkey;     // [n] Morton key by sorted position (meaningful in dense cells)
+  int32_t fbits;
   double ppc_mean;          // generators per grid cell on average (first-radius scaling)
   // periodic image of shift code c = (mx+1) + 3(my+1) + 9(mz+1): the reference's query
   // offset s = (-m) w (rtree_nn.rs:86) and emitted shift -s (rtree_nn.rs:27-33)
@@ -118,6 +121,9 @@ struct Job {
   int64_t rec_cap;
   unsigned long long* rec_counter;
   int64_t* rec_off;         // by sorted position, -1: none
+  // ---- per-warp staging slots of the fused kernel for shells larger than its shared
+  // buffer (slot = global warp index), or nullptr ----
+  char* big;
 };
 
 // One chunk of the staged path: cells at processing positions [item0, item0 + nitems)
@@ -149,6 +155,39 @@ struct Setup {
   double bn[6][3], bp[6][3], bd[6];
   double iloc_a[3], iloc_inv[3];
 };
+
+// Morton keys of the dense-cell octrees: FKEY_BITS bits in all, fkey_bits(dim) per
+// active axis; bit (dim * b + i) of a key is bit b of the sub-cell index along axis i.
+constexpr int FKEY_BITS = 30;
+__host__ __device__ inline int fkey_bits(int dim) { return dim == 3 ? 10 : (dim == 2 ? 15 : 20); }
+__host__ __device__ inline uint32_t spread2(uint32_t v) {  // 10 bits -> every third bit
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ inline uint32_t spread1(uint32_t v) {  // 16 bits -> every other bit
+  v &= 0xffffu;
+  v = (v | (v << 8)) & 0x00ff00ffu;
+  v = (v | (v << 4)) & 0x0f0f0f0fu;
+  v = (v | (v << 2)) & 0x33333333u;
+  v = (v | (v << 1)) & 0x55555555u;
+  return v;
+}
+__host__ __device__ inline uint32_t morton(int dim, uint32_t x, uint32_t y, uint32_t z) {
+  return dim == 3 ? (spread2(x) | (spread2(y) << 1) | (spread2(z) << 2))
+                  : (dim == 2 ? (spread1(x) | (spread1(y) << 1)) : x);
+}
+// Sub-cell index (at the finest level) of coordinate g inside coarse cell c along one axis.
+__host__ __device__ inline uint32_t fine_q(double g, double a, double inv, int c, int bits) {
+  const double top = (double)((1u << bits) - 1u);
+  double t = floor(((g - a) * inv - (double)c) * (double)(1u << bits));
+  if (!(t >= 0.0)) t = 0.0;
+  if (t > top) t = top;
+  return (uint32_t)t;
+}
 
 }  // namespace mv
 

@@ -92,8 +92,13 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     }
     const D3 x = load_gen(J, self);
     bool all = false;
-    const double R = first_radius(J, x);
-    const int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all);
+    double R = first_radius(J, x, lane);
+    int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
+    // too many candidates: pull the radius in, as the fused kernel does
+    for (int shrink = 0; cnt > SHELL_CMAX && shrink < 6; shrink++) {
+      R *= fmin(fmax(cbrt(0.5 * SHELL_CMAX / (double)cnt), 0.1), 0.7);
+      cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
+    }
     if (cnt > SHELL_CMAX || cnt == 0) {
       if (lane == 0) SJ.info[item] = -1;
       continue;
