@@ -79,7 +79,8 @@ typedef struct mv_build_stats {
   int64_t extra_shells;          /* neighbour-shell expansions beyond the first      */
   int64_t overflow_cells;        /* cells re-run in the large capacity tier          */
   int64_t serial_rings;          /* rings rebuilt by the serial fallback             */
-  int64_t staged_retries;        /* staged pipeline: cells rebuilt by the fused kernel */
+  int64_t staged_retries;        /* staged pipeline: cells rebuilt by the fused kernel
+                                  * (those neither staged round closed)              */
   int64_t device_bytes;          /* device workspace held by the context             */
   int64_t kernel_launches;       /* library kernels launched by the build            */
   double ms_grid;                /* device time: generator prep + uniform grid       */
@@ -89,6 +90,8 @@ typedef struct mv_build_stats {
   double ms_clip;                /*   clip kernels                                   */
   double ms_integrate;           /*   integral kernels                               */
   double ms_retry;               /*   fused kernel on the retried cells              */
+  int64_t staged_wide;           /* staged pipeline: cells the first round left to   *
+                                  * the wide (long-list) round                       */
 } mv_build_stats;
 
 /* Device-resident result of a build.  Pointers are owned by the context and stay

@@ -58,7 +58,8 @@ class BuildStats(C.Structure):
         "extra_shells", "overflow_cells", "serial_rings", "staged_retries", "device_bytes",
         "kernel_launches")] + [
         (name, C.c_double) for name in ("ms_grid", "ms_cells", "ms_finalize", "ms_shell",
-                                         "ms_clip", "ms_integrate", "ms_retry")]
+                                         "ms_clip", "ms_integrate", "ms_retry")] + [
+        ("staged_wide", C.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

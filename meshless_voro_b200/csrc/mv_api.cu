@@ -39,6 +39,7 @@ void launch_export_write(const Job& J, const int64_t* rec_by_orig, const double*
 cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st);
 int stage_blocks_per_sm(int kernel, int precision);
 int stage_list_stride();
+int stage_wide_stride();
 int64_t stage_record_words(int np, int nv);
 // mv_grid.cu
 void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
@@ -169,7 +170,7 @@ struct Workspace {
   DevBuf big;  // staging slots of the fused kernel for large shells
   DevBuf counters;
   // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
-  DevBuf cand, cand_info, cand_rad, rec_off, rec, retry, stage_ctr;
+  DevBuf cand, cand_info, cand_rad, rec_off, rec, retry, retry2, stage_ctr;
   // cell export: record per generator, per-cell sizes and offsets, the CSR arrays
   DevBuf x_rec_by_orig, x_cnt, x_off;
   DevBuf x_pn, x_pp, x_pr, x_pc, x_vl, x_vd, x_tv, x_tp, x_fp, x_fvo, x_fv;
@@ -184,7 +185,7 @@ struct mv_context {
   int sm_count = 0;
   int bps_fast[2] = {0, 0};
   int bps_large[2] = {0, 0};
-  int bps_stage[3][2] = {};  // shell, clip, integral kernels by precision
+  int bps_stage[4][2] = {};  // shell, clip, integral, wide-shell kernels by precision
   std::vector<cudaEvent_t> stage_ev;  // 4 per chunk: before shell, clip, integral, after
   double rec_words_hint = 0.0;  // record words per cell the last staged build needed
   Workspace ws;
@@ -271,7 +272,7 @@ int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224
 // receives their number.
 int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& o, int64_t n,
                int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry, double ms_stage[3],
-               unsigned long long* keep_records) {
+               unsigned long long* keep_records, int64_t* n_wide, const int32_t** retry_order) {
   Workspace& W = ctx->ws;
   // an export build keeps every cell's record: one chunk, and the record counter the
   // fused kernel shares (keep_records)
@@ -282,7 +283,13 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
   int64_t wpc = std::max<int64_t>(record_words_per_cell(s.dim), (int64_t)ctx->rec_words_hint);
   wpc = std::min<int64_t>(wpc, stage_record_words(64, 64));
   const int64_t rec_cap = chunk * wpc;
-  const size_t ctr_words = 1 + 3 * (size_t)nchunks;
+  // the wide round re-chunks the retry list so that its longer lists fit the same
+  // candidate buffer
+  const int wstride = stage_wide_stride();
+  const int64_t chunk2 = std::max<int64_t>(1, chunk * stride / wstride);
+  const int64_t nchunks2 = (n + chunk2 - 1) / chunk2;
+  const size_t ctr2 = 1 + 3 * (size_t)nchunks;  // wide-round words start here
+  const size_t ctr_words = ctr2 + 1 + 3 * (size_t)nchunks2;
   int e = 0;
   e |= ensure(ctx, W.cand, 4 * (size_t)chunk * stride);
   e |= ensure(ctx, W.cand_info, 4 * (size_t)chunk);
@@ -290,11 +297,12 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
   e |= ensure(ctx, W.rec_off, 8 * (size_t)chunk);
   e |= ensure(ctx, W.rec, 8 * (size_t)rec_cap);
   e |= ensure(ctx, W.retry, 4 * (size_t)n);
+  if (!keep_records) e |= ensure(ctx, W.retry2, 4 * (size_t)n);
   e |= ensure(ctx, W.stage_ctr, 8 * ctr_words);
   if (e) return MV_ERR_OOM;
   unsigned long long* ctr = P<unsigned long long>(W.stage_ctr);
   MV_CUDA(cudaMemsetAsync(ctr, 0, 8 * ctr_words, st));
-  while (ctx->stage_ev.size() < 4 * (size_t)nchunks) {
+  while (ctx->stage_ev.size() < 4 * (size_t)std::max(nchunks, nchunks2)) {
     cudaEvent_t ev;
     MV_CUDA(cudaEventCreate(&ev));
     ctx->stage_ev.push_back(ev);
@@ -327,9 +335,11 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
   }
   std::vector<unsigned long long> h(ctr_words);
-  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * ctr_words, cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * ctr2, cudaMemcpyDeviceToHost, st));
   MV_CUDA(cudaStreamSynchronize(st));
   *n_retry = (int64_t)(h[0] & 0xffffffffull);
+  *n_wide = 0;
+  *retry_order = P<int32_t>(W.retry);
   for (int k = 0; k < 3; k++) ms_stage[k] = 0.0;
   for (int64_t c = 0; c < nchunks; c++) {
     for (int k = 0; k < 3; k++) {
@@ -337,6 +347,44 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
       cudaEventElapsedTime(&t, ctx->stage_ev[4 * c + k], ctx->stage_ev[4 * c + k + 1]);
       ms_stage[k] += t;
     }
+  }
+  if (!keep_records && *n_retry > 0) {
+    // the wide round over the retry list; what it cannot close goes to the fused kernel
+    const int64_t nr = *n_retry;
+    StageJob SW = SJ;
+    SW.cstride = wstride;
+    SW.order = P<int32_t>(W.retry);
+    SW.retry_list = P<int32_t>(W.retry2);
+    SW.retry_count = reinterpret_cast<unsigned int*>(ctr + ctr2);
+    const int64_t nc = (nr + chunk2 - 1) / chunk2;
+    for (int64_t c = 0; c < nc; c++) {
+      SW.item0 = (int32_t)(c * chunk2);
+      SW.nitems = (int32_t)std::min<int64_t>(chunk2, nr - c * chunk2);
+      SW.work = reinterpret_cast<unsigned int*>(ctr + ctr2 + 1 + 3 * c);
+      SW.rec_counter = ctr + ctr2 + 1 + 3 * c + 2;
+      const int kern[3] = {3, 1, 2};
+      for (int k = 0; k < 3; k++) {
+        int64_t blocks = (int64_t)ctx->sm_count * std::max(1, ctx->bps_stage[kern[k]][pi]);
+        blocks = std::min<int64_t>(blocks, (SW.nitems + 3) / 4);
+        MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + k], st));
+        MV_CUDA(launch_stage(kern[k], J, SW, (int)std::max<int64_t>(1, blocks), st));
+        (*launches)++;
+      }
+      MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
+    }
+    unsigned long long r2 = 0;
+    MV_CUDA(cudaMemcpyAsync(&r2, ctr + ctr2, 8, cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+    for (int64_t c = 0; c < nc; c++) {
+      for (int k = 0; k < 3; k++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ctx->stage_ev[4 * c + k], ctx->stage_ev[4 * c + k + 1]);
+        ms_stage[k] += t;
+      }
+    }
+    *n_wide = nr;
+    *n_retry = (int64_t)(r2 & 0xffffffffull);
+    *retry_order = P<int32_t>(W.retry2);
   }
   // size the record buffer of the next build by what this one asked for
   double need = 0.0;
@@ -632,18 +680,19 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
       J.rec_off = P<int64_t>(W.rec_off);
     }
     bool retry_ran = false;
-    int64_t n_retry = 0;
+    int64_t n_retry = 0, n_wide = 0;
     double ms_stage[3] = {0.0, 0.0, 0.0};
     MV_CUDA(cudaEventRecord(ctx->ev[1], st));
     if (n > 0 && staged) {
+      const int32_t* retry_order = nullptr;
       int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry, ms_stage,
-                           exporting ? &C->rec_counter : nullptr);
+                           exporting ? &C->rec_counter : nullptr, &n_wide, &retry_order);
       if (rc2) return rc2;
       MV_CUDA(cudaEventRecord(ctx->ev[2], st));
       if (n_retry > 0) {
         // cells the first shell did not decide: the fused kernel builds them
         Job Rj = J;
-        Rj.order = P<int32_t>(W.retry);
+        Rj.order = retry_order;
         Rj.n_order = (int32_t)n_retry;
         int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
         blocks = (int)std::min<int64_t>(blocks, (n_retry + 3) / 4);
@@ -663,6 +712,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     ctx->retry_ran = retry_ran;
     stats.staged_retries = n_retry;
+    stats.staged_wide = n_wide;
     stats.ms_shell = ms_stage[0];
     stats.ms_clip = ms_stage[1];
     stats.ms_integrate = ms_stage[2];
@@ -1101,7 +1151,7 @@ int mv_context_create(int device, mv_context** out) {
   for (int p = 0; p < 2; p++) {
     ctx->bps_fast[p] = cells_blocks_per_sm_fast(p);
     ctx->bps_large[p] = cells_blocks_per_sm_large(p);
-    for (int k = 0; k < 3; k++) ctx->bps_stage[k][p] = stage_blocks_per_sm(k, p);
+    for (int k = 0; k < 4; k++) ctx->bps_stage[k][p] = stage_blocks_per_sm(k, p);
   }
   if (cudaGetLastError() != cudaSuccess || ctx->bps_fast[0] <= 0 || ctx->bps_fast[1] <= 0) {
     cudaStreamDestroy(ctx->stream);

@@ -108,7 +108,7 @@ struct Job {
   unsigned long long* face_counter;
   int64_t face_cap;
   // ---- work distribution / retry queue ----
-  int32_t* order;           // sorted positions to process (overflow pass), or nullptr
+  const int32_t* order;     // sorted positions to process (retry / overflow pass), or nullptr
   int32_t n_order;          // number of positions to process
   unsigned int* work_counter;
   int32_t* ovf_list;        // cells that outgrew this capacity tier
@@ -127,10 +127,12 @@ struct Job {
 };
 
 // One chunk of the staged path: cells at processing positions [item0, item0 + nitems)
-// go through the shell, clip and integral kernels.
+// go through the shell, clip and integral kernels.  The first round processes the
+// cells in grid order; the second (wide) round takes the first round's retry list.
 struct StageJob {
   int32_t item0;
   int32_t nitems;
+  const int32_t* order;       // processing position -> sorted position, or nullptr (identity)
   int32_t cstride;            // candidate-list entries per cell
   uint32_t* cand;             // [nitems][cstride]: sorted position * 27 + shift code
   int32_t* info;              // [nitems]: count | exhausted << 30, 0: inactive, -1: retry

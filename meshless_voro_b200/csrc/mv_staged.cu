@@ -33,6 +33,7 @@ namespace mv {
 #define MV_CLIP_WARPS 4
 #endif
 constexpr int SHELL_CMAX = 128;
+constexpr int SHELL_MIN = 64;  // first shells below this many candidates are widened
 constexpr int SHELL_WARPS = 4;
 #ifndef MV_SHELL_MINB
 #define MV_SHELL_MINB 8
@@ -43,6 +44,11 @@ constexpr int INT_WARPS = 4;
 #define MV_INT_MINB 8
 #endif
 using TierClip = Tier<64, 64, SHELL_CMAX, 8, uint8_t, MV_CLIP_MINB>;
+
+// sorted position of processing item `item` of a chunk
+__device__ __forceinline__ int stage_pos(const StageJob& SJ, int item) {
+  return SJ.order != nullptr ? __ldg(SJ.order + SJ.item0 + item) : SJ.item0 + item;
+}
 
 // ------------------------------------------------------------------- shell --
 // Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     if (lane == 0) item = (int)atomicAdd(SJ.work + 0, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= SJ.nitems) break;
-    const int spos = SJ.item0 + item;
+    const int spos = stage_pos(SJ, item);
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       if (lane == 0) SJ.info[item] = 0;
@@ -94,9 +100,18 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     bool all = false;
     double R = first_radius(J, x, lane);
     int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
-    // too many candidates: pull the radius in, as the fused kernel does
-    for (int shrink = 0; cnt > SHELL_CMAX && shrink < 6; shrink++) {
-      R *= fmin(fmax(cbrt(0.5 * SHELL_CMAX / (double)cnt), 0.1), 0.7);
+    // the density estimate behind R is rough where the density varies: a shell that
+    // overflows the list is pulled in, one far below a uniform region's ~92 candidates
+    // (too small to close most cells) is widened, a few times at most
+    for (int it = 0; it < 6; it++) {
+      double f;
+      if (cnt > SHELL_CMAX)
+        f = fmin(fmax(cbrt(0.6 * SHELL_CMAX / (double)cnt), 0.1), 0.9);
+      else if (cnt < SHELL_MIN && !all)
+        f = fmin(cbrt(96.0 / (double)max(cnt, 1)), 2.0);
+      else
+        break;
+      R *= f;
       cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
     }
     if (cnt > SHELL_CMAX || cnt == 0) {
@@ -114,6 +129,65 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
     // fused kernel reports the error otherwise
     if (lane == 0) {
+      SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
+      SJ.rad[item] = R;
+    }
+    __syncwarp();
+  }
+}
+
+// The wide round: cells the first round could not close get a shell of up to WIDE_CMAX
+// candidates (about eight times the first one), sorted in shared memory.  Cells the
+// wide round cannot close either go to the fused kernel.
+constexpr int WIDE_CMAX = 1024;
+constexpr int WIDE_MIN = 384;
+constexpr int WIDE_WARPS = 4;
+constexpr size_t WIDE_SMEM = sizeof(ShellBuf<WIDE_CMAX>) * WIDE_WARPS;
+
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, 3) shell_wide_kernel(const __grid_constant__ Job J,
+                                                                 const __grid_constant__ StageJob SJ) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double ext_s[6];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  ShellBuf<WIDE_CMAX>& B = reinterpret_cast<ShellBuf<WIDE_CMAX>*>(smem_raw)[warp];
+  if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  __syncthreads();
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(SJ.work + 0, 1u);
+    item = __shfl_sync(FULL, item, 0);
+    if (item >= SJ.nitems) break;
+    const int spos = stage_pos(SJ, item);
+    const int self = __ldg(J.sid + spos);
+    if (J.mask != nullptr && J.mask[self] == 0) {
+      if (lane == 0) SJ.info[item] = 0;
+      continue;
+    }
+    const D3 x = load_gen(J, self);
+    bool all = false;
+    double R = 2.0 * first_radius(J, x, lane);
+    int cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 4 * WIDE_CMAX);
+    for (int it = 0; it < 6; it++) {
+      double f;
+      if (cnt > WIDE_CMAX)
+        f = fmin(fmax(cbrt(0.6 * WIDE_CMAX / (double)cnt), 0.1), 0.9);
+      else if (cnt < WIDE_MIN && !all)
+        f = fmin(cbrt(0.75 * WIDE_CMAX / (double)max(cnt, 1)), 2.0);
+      else
+        break;
+      R *= f;
+      cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 4 * WIDE_CMAX);
+    }
+    if (cnt > WIDE_CMAX || cnt == 0) {
+      if (lane == 0) SJ.info[item] = -1;
+      continue;
+    }
+    sort_shell<WIDE_CMAX>(B, lane, cnt);
+    uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
+    for (int i = lane; i < cnt; i += 32) out[i] = (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u;
+    if (lane == 0) {
+      const bool self_first = (int)(B.tie[0] / 27u) == self;
       SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
       SJ.rad[item] = R;
     }
@@ -464,7 +538,7 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
     if (lane == 0) item = (int)atomicAdd(SJ.work + 1, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= SJ.nitems) break;
-    const int spos = SJ.item0 + item;
+    const int spos = stage_pos(SJ, item);
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       // VoronoiCell::default() (voronoi.rs:303-305)
@@ -524,7 +598,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(cons
     if (item >= SJ.nitems) break;
     const int64_t off = SJ.rec_off[item];
     if (off < 0) continue;
-    const int spos = SJ.item0 + item;
+    const int spos = stage_pos(SJ, item);
     const int self = __ldg(J.sid + spos);
     const D3 x = load_gen(J, self);
     const RecordView V(SJ.rec + off);
@@ -560,6 +634,7 @@ constexpr size_t CLIP_SMEM = sizeof(ClipSmem<TierClip>) * CLIP_WARPS;
 
 int stage_blocks_per_sm(int kernel, int precision) {
   if (kernel == 0) return occupancy(shell_kernel<SHELL_WARPS>, 32 * SHELL_WARPS, 0);
+  if (kernel == 3) return occupancy(shell_wide_kernel<WIDE_WARPS>, 32 * WIDE_WARPS, WIDE_SMEM);
   if (kernel == 1)
     return precision == MV_PRECISION_FILTERED
                ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>, 32 * CLIP_WARPS,
@@ -570,6 +645,7 @@ int stage_blocks_per_sm(int kernel, int precision) {
 }
 
 int stage_list_stride() { return SHELL_CMAX; }
+int stage_wide_stride() { return WIDE_CMAX; }
 
 int64_t stage_record_words(int np, int nv) { return rec_words(np, nv); }
 
@@ -577,6 +653,11 @@ cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int block
   if (blocks < 1) blocks = 1;
   if (kernel == 0) {
     shell_kernel<SHELL_WARPS><<<blocks, 32 * SHELL_WARPS, 0, st>>>(J, SJ);
+  } else if (kernel == 3) {
+    auto k = shell_wide_kernel<WIDE_WARPS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WIDE_SMEM);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, 32 * WIDE_WARPS, WIDE_SMEM, st>>>(J, SJ);
   } else if (kernel == 1) {
     if (J.precision == MV_PRECISION_FILTERED) {
       auto k = clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>;

@@ -69,6 +69,12 @@ def _case(name):
     if name == "clustered_2d_periodic":
         return dict(generators=W.clustered(12000, 30, seed=13, dim=2)["generators"],
                     anchor=[0, 0, 0], width=[1, 1, 1], dim=2, periodic=True)
+    if name == "clump6k_in_3k_periodic":
+        # a compact clump in a sparse background: the safety radius of every cell on
+        # the clump's surface takes in the whole clump (more than either staged list)
+        g = np.concatenate([rng.uniform(0, 1, (3000, 3)),
+                            np.mod([0.37, 0.52, 0.61] + 1e-3 * rng.standard_normal((6000, 3)), 1.0)])
+        return dict(generators=g, anchor=[0, 0, 0], width=[1, 1, 1], dim=3, periodic=True)
     if name == "degenerate_2e15":
         g = W.perturbed_grid([0, 0, 0], [2e15] * 3, 10, 0.0, None)
         g[42] = 1e14 * np.array([1.00007490802, 9.00019014286, 5.00014639879])
@@ -80,7 +86,7 @@ CASES = ["single", "two", "five_2d", "four_2d_periodic", "lattice4_rect", "latti
          "jitter16_rect", "grid15_w2", "poisson20k_periodic", "poisson5k_rect_aniso",
          "small_periodic_17", "plane25_periodic_2d", "poisson_2d_rect", "line_1d_periodic",
          "non_perturbed_z", "degenerate_2e15", "clustered30k_periodic", "clustered20k_rect",
-         "clustered_2d_periodic"]
+         "clustered_2d_periodic", "clump6k_in_3k_periodic"]
 
 
 def _rel_err(a, b, scale):
@@ -174,10 +180,30 @@ def test_staged_retry_and_stats(gpu_ctx, oracle, precision):
                                    precision=precision, **kw)
         assert compare(gpu, orc)
         stats[pipe] = gpu_ctx.last_stats()
-    assert stats["staged"]["staged_retries"] > 0
-    assert stats["fused"]["staged_retries"] == 0
+    assert stats["staged"]["staged_retries"] + stats["staged"]["staged_wide"] > 0
+    assert stats["fused"]["staged_retries"] == 0 and stats["fused"]["staged_wide"] == 0
     for k in ("cells_built", "neighbours_clipped", "planes_added", "exact_tests", "serial_rings"):
         assert stats["staged"][k] == stats["fused"][k], k
+
+
+@pytest.mark.parametrize("precision", ["filtered", "fp64"])
+def test_staged_rounds_and_fused_fallback(gpu_ctx, oracle, precision):
+    """Cells around a compact clump need more neighbours than the first staged list
+    (the wide round takes them) and than the wide list (the fused kernel's staged big
+    shells take them); every cell must come out as the oracle builds it."""
+    c = _case("clump6k_in_3k_periodic")
+    orc = oracle.build(c["generators"], c["anchor"], c["width"], dim=3, periodic=True)
+    gpu = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], 3, True,
+                               precision=precision, pipeline="staged", chunk_cells=2048)
+    assert compare(gpu, orc)
+    st = gpu_ctx.last_stats()
+    assert st["staged_wide"] > 0 and st["staged_retries"] > 0
+    fused = gpu_ctx.build_arrays(c["generators"], None, c["anchor"], c["width"], 3, True,
+                                 precision=precision, pipeline="fused")
+    assert compare(fused, orc)
+    sf = gpu_ctx.last_stats()
+    for k in ("cells_built", "neighbours_clipped", "planes_added", "exact_tests", "serial_rings"):
+        assert st[k] == sf[k], k
 
 
 def test_reference_api_kats(gpu_ctx):
