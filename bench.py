@@ -7,7 +7,8 @@ ordering and the cell -> face CSR.  Default workload: 256^3 = 16,777,216 i.i.d.
 uniform generators in the periodic unit box (seeded, synthetic).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision filtered|fp64]
-                  [--workload poisson_256|lattice_64|jitter_32|clustered] [--impl ours|reference]
+                  [--workload poisson_256|lattice_64|jitter_32|clustered|batch_4096]
+                  [--impl ours|reference]
                   [--pipeline auto|staged|fused]
 
 The default pipeline runs the staged shell / clip / integral kernels; the plain FP64
@@ -83,6 +84,162 @@ def workload(name: str, seed: int):
     else:
         raise SystemExit(f"unknown workload {name}")
     return w
+
+
+BATCH_GROUP_CELLS = 1 << 25  # generators per batch build (device memory bound)
+
+
+def batch_groups(jobs, cap=BATCH_GROUP_CELLS):
+    """Consecutive groups of jobs with at most `cap` generators each (a job larger than
+    cap forms its own group)."""
+    groups, cur, m = [], [], 0
+    for j in jobs:
+        k = len(j["generators"])
+        if cur and m + k > cap:
+            groups.append(cur)
+            cur, m = [], 0
+        cur.append(j)
+        m += k
+    if cur:
+        groups.append(cur)
+    return groups
+
+
+def cpu_baseline_batch(jobs, budget_s=12.0, threads=None):
+    """The oracle on all host cores, one tessellation after another (as a caller of the
+    reference loops over Voronoi::build), over the batch's first jobs for about
+    budget_s seconds; cells/s extrapolated to the batch."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    cells, t, k = 0, 0.0, 0
+    for j in jobs:
+        t0 = time.perf_counter()
+        r = O.build(j["generators"], j["anchor"], j["width"], dim=j["dimensionality"],
+                    periodic=j["periodic"], mask=j.get("mask"), nthreads=threads, flags=O.NO_CSR)
+        assert r.status == 0
+        t += time.perf_counter() - t0
+        cells += len(j["generators"])
+        k += 1
+        if t >= budget_s:
+            break
+    return {"value": cells / t, "unit": "cells/s", "cores": threads, "kind": "port",
+            "sample": f"the first {k} of the {len(jobs)} tessellations ({cells} cells, "
+                      f"{t:.1f} s), one build per tessellation"}
+
+
+def run_batch(args, rank, world):
+    """Batched uneven tessellations: every step builds all jobs (in groups of at most
+    BATCH_GROUP_CELLS generators, one mv_context_build_batch_device call each)."""
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    import meshless_voro_b200 as mv
+    from meshless_voro_b200 import _native as NN
+    from meshless_voro_b200 import workloads as W
+    from meshless_voro_b200.voronoi import batch_inputs
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev,
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    njobs = int(args.workload.split("_")[1])
+    jobs = W.batch_jobs(njobs=njobs, seed=rank_seed(rank))
+    n = sum(len(j["generators"]) for j in jobs)
+    groups = []
+    for grp in batch_groups(jobs):
+        g, m, descs = batch_inputs(grp)
+        gh = torch.from_numpy(g).pin_memory()
+        mh = torch.from_numpy(m).pin_memory() if m is not None else None
+        groups.append(dict(gh=gh, mh=mh, gd=gh.to(dev), md=mh.to(dev) if mh is not None else None,
+                           descs=descs, n=len(g)))
+    ctx = mv.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        stats, F, Cn = [], 0, 0
+        for gr in groups:
+            out = ctx.build_batch_device(gr["gd"].data_ptr(), gr["md"].data_ptr() if gr["md"] is not None else 0,
+                                         gr["descs"], precision=args.precision, stream=sp)
+            F += int(out.n_faces)
+            Cn += int(out.n_connections)
+            stats.append(ctx.last_stats())
+        return stats, F, Cn
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev), r
+
+    with ClockSampler(local) as clk:
+        ms, (stats, F, Cn) = timed(step)
+    clocks = clk.summary()
+    value = aggregate_cells_per_s(world, n, ms)
+
+    e2e = None
+    if not args.no_e2e:
+        opts = mv.voronoi.make_options(args.precision, stream=sp)
+
+        def e2e_step():
+            d2h = 0
+            for gr in groups:
+                bv = NN.BatchVoronoi()
+                rc = NN.lib().mv_context_build_batch(
+                    ctx.handle, C.c_void_p(gr["gh"].data_ptr()),
+                    C.c_void_p(gr["mh"].data_ptr()) if gr["mh"] is not None else None,
+                    gr["descs"], len(gr["descs"]), C.byref(opts), C.byref(bv))
+                NN.check(rc)
+                d2h += 52 * gr["n"] + 65 * int(bv.n_faces) + 4 * int(bv.n_connections)
+            return d2h
+
+        e_ms, d2h = timed(e2e_step)
+        h2d = sum(24 * gr["n"] + (gr["n"] if gr["mh"] is not None else 0) for gr in groups)
+        e2e = {"value": aggregate_cells_per_s(world, n, e_ms), "unit": "cells/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
+
+    peak, peak_kind = measured_peaks()
+    cells_ms = sum(st["ms_cells"] for st in stats)
+    alg_bytes = BYTES_GEN * n + BYTES_CELL * n + BYTES_FACE * F + BYTES_CONN * Cn
+    achieved = alg_bytes / (cells_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "kernel": "all cell kernels of the batch builds",
+                "alg_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": cells_ms}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline_batch(jobs, budget_s=args.cpu_budget)
+    if rank == 0:
+        tot = lambda k: int(sum(st[k] for st in stats))
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"batch_{njobs}_uneven_tessellations", "n_jobs": njobs,
+                           "n_generators": n, "batch_builds_per_step": len(groups),
+                           "precision": args.precision, "parallelism": f"weak{world}",
+                           "cache": "inputs larger than L2"},
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
+                "gpu_launches": tot("kernel_launches") * args.steps, "clocks": clocks,
+                "phases_ms": {"grid": sum(st["ms_grid"] for st in stats), "cells": cells_ms,
+                              "finalize": sum(st["ms_finalize"] for st in stats)},
+                "counts": {"faces": F, "connections": Cn, "cells_built": tot("cells_built"),
+                           "staged_wide": tot("staged_wide"), "staged_retries": tot("staged_retries"),
+                           "overflow_cells": tot("overflow_cells")}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def measured_peaks():
@@ -184,6 +341,26 @@ def cpu_baseline(w, budget_s=12.0, threads=None):
 def run_reference(args, rank, world):
     if rank != 0:
         return
+    if args.workload.startswith("batch_"):
+        from meshless_voro_b200 import workloads as W
+        jobs = W.batch_jobs(njobs=int(args.workload.split("_")[1]), seed=rank_seed(0))
+        for _ in range(args.warmup):
+            cpu_baseline_batch(jobs[:4], budget_s=1.0)
+        vals, cb = [], None
+        for _ in range(args.steps):
+            cb = cpu_baseline_batch(jobs, budget_s=args.cpu_budget)
+            vals.append(cb["value"])
+        v = float(np.median(vals))
+        n = sum(len(j["generators"]) for j in jobs)
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic", "impl": "reference",
+                          "config": {"workload": args.workload, "n_generators": n},
+                          "cpu_baseline": {**cb, "value": v},
+                          "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
     w = workload(args.workload, seed=3)
     n = len(w["generators"])
     vals = []
@@ -229,6 +406,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload.startswith("batch_"):
+        run_batch(args, rank, world)
         return
 
     import torch

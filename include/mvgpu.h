@@ -236,6 +236,68 @@ int mv_context_build_cells(mv_context* ctx, const double* generators, const uint
                            int dimensionality, int periodic, const mv_options* opts,
                            int cells_flags, mv_voronoi** voronoi, mv_cells** cells);
 
+/* ---- batches: many tessellations in one build ----
+ *
+ * The reference builds one tessellation per call (Voronoi::build, voronoi.rs:151-238);
+ * a caller with many independent tessellations (uneven sizes, mixed dimensionality,
+ * periodic and rectangular, full and partial) calls it in a loop.  A batch build does
+ * them together: one grid build, one pass of the cell kernels over all cells (each
+ * cell finds its tessellation), one finalize, so the launch count does not grow with
+ * the number of tessellations and small tessellations share the GPU.  Each
+ * tessellation's result is exactly what mv_context_build_device returns for it alone.
+ *
+ * Inputs are concatenated: tessellation j's generators are the rows
+ * [sum_{i<j} n_i, sum_{i<=j} n_i) of one [sum n][3] array (and of one mask array,
+ * used for the tessellations with has_mask set). */
+typedef struct mv_job {
+  int64_t n;                 /* generators of the tessellation                        */
+  double anchor[3];          /* simulation box, as Voronoi::build's anchor / width    */
+  double width[3];
+  int32_t dimensionality;    /* 1, 2 or 3                                             */
+  int32_t periodic;
+  int32_t has_mask;          /* build_partial: the tessellation's mask rows apply     */
+  int32_t reserved;
+} mv_job;
+
+/* Result of a batch: the tessellations' results concatenated, each in the reference's
+ * own indexing (cell and face indices local to the tessellation; cell_face_offset
+ * relative to the tessellation's first connection).  Tessellation j owns cells
+ * [job_cell_offset[j], job_cell_offset[j+1]), faces [job_face_offset[j], ...) and
+ * connections [job_connection_offset[j], ...).  The offset arrays are host memory;
+ * the other arrays are device memory for mv_context_build_batch_device and pinned
+ * host memory for mv_context_build_batch.  All are owned by the context and valid
+ * until its next build.  On an error status error_job / error_cell name the first
+ * failing tessellation and its cell. */
+typedef struct mv_batch_voronoi {
+  int64_t n_jobs, n_cells, n_faces, n_connections;
+  const int64_t* job_cell_offset;        /* [n_jobs + 1] */
+  const int64_t* job_face_offset;        /* [n_jobs + 1] */
+  const int64_t* job_connection_offset;  /* [n_jobs + 1] */
+  double* cell_volume;
+  double* cell_centroid;
+  double* cell_safety_radius;
+  int64_t* cell_face_offset;
+  int32_t* cell_face_count;
+  int32_t* face_left;
+  int32_t* face_right;
+  double* face_area;
+  double* face_centroid;
+  double* face_normal;
+  uint8_t* face_shift_code;
+  int32_t* cell_face_connections;
+  int64_t error_job, error_cell;
+} mv_batch_voronoi;
+
+/* Batch build from device inputs (d_mask may be NULL when no job has has_mask). */
+int mv_context_build_batch_device(mv_context* ctx, const double* d_generators, const uint8_t* d_mask,
+                                  const mv_job* jobs, int64_t n_jobs, const mv_options* opts,
+                                  mv_batch_voronoi* out);
+
+/* Batch build from host inputs, results copied to the context's pinned host arena. */
+int mv_context_build_batch(mv_context* ctx, const double* generators, const uint8_t* mask,
+                           const mv_job* jobs, int64_t n_jobs, const mv_options* opts,
+                           mv_batch_voronoi* out);
+
 /* ---- build without allocating (no counterpart in the reference crate) ----
  *
  * For callers that cannot call cudaMalloc -- a host framework that has handed all

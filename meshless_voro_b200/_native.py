@@ -42,7 +42,7 @@ EXPORTED = (
     "mv_context_destroy", "mv_context_last_stats", "mv_context_build_device",
     "mv_context_build", "mv_voronoi_build", "mv_voronoi_build_partial", "mv_voronoi_free",
     "mv_shift_from_code", "mv_voronoi_build_noalloc", "mv_context_build_cells_device",
-    "mv_context_build_cells",
+    "mv_context_build_cells", "mv_context_build_batch_device", "mv_context_build_batch",
 )
 
 
@@ -107,6 +107,24 @@ class Cells(C.Structure):
         ("face_vertices", C.c_void_p)]
 
 
+class Job(C.Structure):
+    """mv_job: one tessellation of a batch (its rows of the concatenated inputs)."""
+    _fields_ = [("n", C.c_int64), ("anchor", C.c_double * 3), ("width", C.c_double * 3),
+                ("dimensionality", C.c_int32), ("periodic", C.c_int32), ("has_mask", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class BatchVoronoi(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in ("n_jobs", "n_cells", "n_faces", "n_connections")] + [
+        (name, C.POINTER(C.c_int64)) for name in (
+            "job_cell_offset", "job_face_offset", "job_connection_offset")] + [
+        (name, C.c_void_p) for name in (
+            "cell_volume", "cell_centroid", "cell_safety_radius", "cell_face_offset",
+            "cell_face_count", "face_left", "face_right", "face_area", "face_centroid",
+            "face_normal", "face_shift_code", "cell_face_connections")] + [
+        ("error_job", C.c_int64), ("error_cell", C.c_int64)]
+
+
 _lib = None
 
 
@@ -164,6 +182,14 @@ def lib():
             C.POINTER(Options), C.c_int, C.POINTER(C.POINTER(HostVoronoi)),
             C.POINTER(C.POINTER(Cells))]
         L.mv_context_build_cells.restype = C.c_int
+        L.mv_context_build_batch_device.argtypes = [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Job), C.c_int64, C.POINTER(Options),
+            C.POINTER(BatchVoronoi)]
+        L.mv_context_build_batch_device.restype = C.c_int
+        L.mv_context_build_batch.argtypes = [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Job), C.c_int64, C.POINTER(Options),
+            C.POINTER(BatchVoronoi)]
+        L.mv_context_build_batch.restype = C.c_int
         _lib = L
     return _lib
 

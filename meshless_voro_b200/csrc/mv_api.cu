@@ -20,7 +20,7 @@
 
 namespace mv {
 // mv_cells.cu
-cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
+cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st, const JobTable& TB);
 size_t cells_big_bytes(int blocks_fast, int blocks_large);
 int cells_blocks_per_sm_fast(int precision);
 int cells_blocks_per_sm_large(int precision);
@@ -36,7 +36,8 @@ void launch_export_write(const Job& J, const int64_t* rec_by_orig, const double*
                          int32_t* face_plane, int64_t* face_vert_off, int32_t* face_verts,
                          int64_t n_faces, int64_t n_face_verts, int32_t* status, cudaStream_t st);
 // mv_staged.cu
-cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st);
+cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, const JobTable& TB, int blocks,
+                         cudaStream_t st);
 int stage_blocks_per_sm(int kernel, int precision);
 int stage_list_stride();
 int stage_wide_stride();
@@ -48,6 +49,24 @@ void launch_grid_coarse(const double* gen, int n, const int G[3], const double a
                         const double inv[3], int32_t* cid, int32_t* count, int32_t* start,
                         int32_t* dflag, int32_t* dprefix, int dim, long long* scan_tmp, cudaStream_t st);
 size_t grid_dense_sort_bytes(int n, int64_t ncell);
+void launch_batch_grid(const double* xyz, int n, const int32_t* pos, const int32_t* cbase, int nj,
+                       const BatchGrid* bg, int64_t ncell, double* gen, unsigned long long* ext_keys,
+                       double* ext, int* bad, int32_t* cid, int32_t* count, int32_t* start,
+                       int32_t* dflag, int32_t* dprefix, long long* scan_tmp, cudaStream_t st);
+cudaError_t launch_batch_sort(const double* gen, int n, const int32_t* pos, const int32_t* cbase, int nj,
+                              const BatchGrid* bg, int64_t ncell, const int32_t* cid, const int32_t* dflag,
+                              unsigned long long* key_a, unsigned long long* key_b, int32_t* val_a,
+                              int32_t* val_b, void* sort_tmp, size_t sort_bytes, double* sx, double* sy,
+                              double* sz, int32_t* sid, uint32_t* fkey, int32_t* start, cudaStream_t st);
+void launch_batch_csr(const FaceArrays& f, int64_t F, const int64_t* face_off, const int32_t* face_count,
+                      int n, const int32_t* pos, int nj, int32_t* in_count, int32_t* conn_count,
+                      cudaStream_t st);
+void launch_batch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, const int64_t* conn_off,
+                           const int32_t* in_count, int32_t* cursor, int n, const int32_t* pos, int nj,
+                           int32_t* conn, cudaStream_t st);
+void launch_batch_localize(FaceArrays& f, int64_t F, const int64_t* face_off, int64_t* conn_off,
+                           const int32_t* conn_count, int32_t* conn, int n, const int32_t* pos, int nj,
+                           int64_t* fbase, int64_t* cbase_conn, cudaStream_t st);
 cudaError_t launch_grid_dense(const double* gen, int n, const int G[3], const double a[3],
                               const double inv[3], int dim, const int32_t* cid, const int32_t* dflag,
                               unsigned long long* key_a, unsigned long long* key_b, int32_t* val_a,
@@ -168,6 +187,8 @@ struct Workspace {
   DevBuf f_left, f_right, f_area, f_cen, f_nrm, f_code;
   DevBuf ovf_a, ovf_b;
   DevBuf big;  // staging slots of the fused kernel for large shells
+  // batches: job table, bases, per-tessellation grids and extents
+  DevBuf b_jobs, b_pos, b_cbase, b_grid, b_ext_keys, b_ext, b_fbase, b_cbconn;
   DevBuf counters;
   // staged pipeline: candidate lists, cell records, retry list, per-chunk counters
   DevBuf cand, cand_info, cand_rad, rec_off, rec, retry, retry2, stage_ctr;
@@ -198,6 +219,8 @@ struct mv_context {
   void* host = nullptr;
   size_t host_cap = 0;
   mv_voronoi hv{};
+  // host offsets of the last batch build
+  std::vector<int64_t> bj_cell, bj_face, bj_conn;
   // pinned host arena for the cells of mv_context_build_cells
   void* host_cells = nullptr;
   size_t host_cells_cap = 0;
@@ -270,9 +293,10 @@ int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224
 // Shell, clip and integral kernels over chunks of cells in processing (grid) order.
 // Cells the first shell does not decide are appended to the retry list; *n_retry
 // receives their number.
-int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& o, int64_t n,
-               int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry, double ms_stage[3],
-               unsigned long long* keep_records, int64_t* n_wide, const int32_t** retry_order) {
+int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const mv_options& o,
+               int64_t n, int pi, cudaStream_t st, int64_t* launches, int64_t* n_retry,
+               double ms_stage[3], unsigned long long* keep_records, int64_t* n_wide,
+               const int32_t** retry_order) {
   Workspace& W = ctx->ws;
   // an export build keeps every cell's record: one chunk, and the record counter the
   // fused kernel shares (keep_records)
@@ -280,7 +304,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
                                      : std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
   const int64_t nchunks = (n + chunk - 1) / chunk;
   const int stride = stage_list_stride();
-  int64_t wpc = std::max<int64_t>(record_words_per_cell(s.dim), (int64_t)ctx->rec_words_hint);
+  int64_t wpc = std::max<int64_t>(record_words_per_cell(dim), (int64_t)ctx->rec_words_hint);
   wpc = std::min<int64_t>(wpc, stage_record_words(64, 64));
   const int64_t rec_cap = chunk * wpc;
   // the wide round re-chunks the retry list so that its longer lists fit the same
@@ -329,7 +353,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
       int64_t blocks = (int64_t)ctx->sm_count * std::max(1, ctx->bps_stage[k][pi]);
       blocks = std::min<int64_t>(blocks, (warps_needed + wpb - 1) / wpb);
       MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + k], st));
-      MV_CUDA(launch_stage(k, J, SJ, (int)std::max<int64_t>(1, blocks), st));
+      MV_CUDA(launch_stage(k, J, SJ, TB, (int)std::max<int64_t>(1, blocks), st));
       (*launches)++;
     }
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
@@ -367,7 +391,7 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
         int64_t blocks = (int64_t)ctx->sm_count * std::max(1, ctx->bps_stage[kern[k]][pi]);
         blocks = std::min<int64_t>(blocks, (SW.nitems + 3) / 4);
         MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + k], st));
-        MV_CUDA(launch_stage(kern[k], J, SW, (int)std::max<int64_t>(1, blocks), st));
+        MV_CUDA(launch_stage(kern[k], J, SW, TB, (int)std::max<int64_t>(1, blocks), st));
         (*launches)++;
       }
       MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
@@ -393,6 +417,79 @@ int run_staged(mv_context* ctx, const Job& J, const Setup& s, const mv_options& 
     need = std::max(need, (double)h[1 + 3 * c + 2] / (double)std::max<int64_t>(items, 1));
   }
   if (!keep_records && need * 1.1 > (double)wpc) ctx->rec_words_hint = need * 1.2;
+  return MV_OK;
+}
+
+// The cell phase of a build, after the grid: the staged rounds (or the fused kernel
+// alone), the fused kernel on what they left, the large tier on the cells that outgrew
+// the fast one; reads the device counters back into *hc.  J is the build's Job (for a
+// batch, the template Job whose shared fields all tessellations use; TB its job table).
+int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const mv_options& o,
+                   int64_t n, int pi, bool staged, bool exporting, cudaStream_t st, int64_t* launches,
+                   mv_build_stats* stats, DevCounters* hc) {
+  Workspace& W = ctx->ws;
+  DevCounters* C = P<DevCounters>(W.counters);
+  bool retry_ran = false;
+  int64_t n_retry = 0, n_wide = 0;
+  double ms_stage[3] = {0.0, 0.0, 0.0};
+  MV_CUDA(cudaEventRecord(ctx->ev[1], st));
+  if (n > 0 && staged) {
+    const int32_t* retry_order = nullptr;
+    int rc2 = run_staged(ctx, J, TB, dim, o, n, pi, st, launches, &n_retry, ms_stage,
+                         exporting ? &C->rec_counter : nullptr, &n_wide, &retry_order);
+    if (rc2) return rc2;
+    MV_CUDA(cudaEventRecord(ctx->ev[2], st));
+    if (n_retry > 0) {
+      // cells neither staged round closed: the fused kernel builds them
+      Job Rj = J;
+      Rj.order = retry_order;
+      Rj.n_order = (int32_t)n_retry;
+      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+      blocks = (int)std::min<int64_t>(blocks, (n_retry + 3) / 4);
+      MV_CUDA(cudaEventRecord(ctx->ev[7], st));
+      MV_CUDA(launch_cells(Rj, false, blocks, st, TB));
+      MV_CUDA(cudaEventRecord(ctx->ev[8], st));
+      (*launches)++;
+      retry_ran = true;
+    }
+  } else {
+    if (n > 0) {
+      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+      MV_CUDA(launch_cells(J, false, blocks, st, TB));
+      (*launches)++;
+    }
+    MV_CUDA(cudaEventRecord(ctx->ev[2], st));
+  }
+  ctx->retry_ran = retry_ran;
+  stats->staged_retries = n_retry;
+  stats->staged_wide = n_wide;
+  stats->ms_shell = ms_stage[0];
+  stats->ms_clip = ms_stage[1];
+  stats->ms_integrate = ms_stage[2];
+  bool large_ran = false;
+  MV_CUDA(cudaMemcpyAsync(hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaStreamSynchronize(st));
+  if (hc->bad_input) return MV_ERR_ARG;
+  const unsigned novf = hc->ovf_count[0];
+  if (novf > 0 && !hc->status[STATUS_CODE]) {
+    // cells that outgrew the fast tier: the large tier rebuilds them
+    Job L = J;
+    L.order = P<int32_t>(W.ovf_a);
+    L.n_order = (int32_t)novf;
+    L.work_counter = &C->work[1];
+    L.ovf_list = P<int32_t>(W.ovf_b);
+    L.ovf_count = &C->ovf_count[1];
+    int blocks = ctx->sm_count * std::max(1, ctx->bps_large[pi]);
+    blocks = std::min<int>(blocks, (int)novf);
+    MV_CUDA(cudaEventRecord(ctx->ev[3], st));
+    MV_CUDA(launch_cells(L, true, blocks, st, TB));
+    MV_CUDA(cudaEventRecord(ctx->ev[4], st));
+    (*launches)++;
+    large_ran = true;
+    MV_CUDA(cudaMemcpyAsync(hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+  }
+  ctx->large_ran = large_ran;
   return MV_OK;
 }
 
@@ -679,68 +776,12 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
       J.rec_counter = &C->rec_counter;
       J.rec_off = P<int64_t>(W.rec_off);
     }
-    bool retry_ran = false;
-    int64_t n_retry = 0, n_wide = 0;
-    double ms_stage[3] = {0.0, 0.0, 0.0};
-    MV_CUDA(cudaEventRecord(ctx->ev[1], st));
-    if (n > 0 && staged) {
-      const int32_t* retry_order = nullptr;
-      int rc2 = run_staged(ctx, J, s, o, n, pi, st, &launches, &n_retry, ms_stage,
-                           exporting ? &C->rec_counter : nullptr, &n_wide, &retry_order);
-      if (rc2) return rc2;
-      MV_CUDA(cudaEventRecord(ctx->ev[2], st));
-      if (n_retry > 0) {
-        // cells the first shell did not decide: the fused kernel builds them
-        Job Rj = J;
-        Rj.order = retry_order;
-        Rj.n_order = (int32_t)n_retry;
-        int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
-        blocks = (int)std::min<int64_t>(blocks, (n_retry + 3) / 4);
-        MV_CUDA(cudaEventRecord(ctx->ev[7], st));
-        MV_CUDA(launch_cells(Rj, false, blocks, st));
-        MV_CUDA(cudaEventRecord(ctx->ev[8], st));
-        launches++;
-        retry_ran = true;
-      }
-    } else {
-      if (n > 0) {
-        int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
-        MV_CUDA(launch_cells(J, false, blocks, st));
-        launches++;
-      }
-      MV_CUDA(cudaEventRecord(ctx->ev[2], st));
-    }
-    ctx->retry_ran = retry_ran;
-    stats.staged_retries = n_retry;
-    stats.staged_wide = n_wide;
-    stats.ms_shell = ms_stage[0];
-    stats.ms_clip = ms_stage[1];
-    stats.ms_integrate = ms_stage[2];
-    bool large_ran = false;
     DevCounters hc;
-    MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
-    if (hc.bad_input) return MV_ERR_ARG;
-    unsigned novf = hc.ovf_count[0];
-    if (novf > 0 && !hc.status[STATUS_CODE]) {
-      // cells that outgrew the fast tier: the large tier rebuilds them
-      Job L = J;
-      L.order = P<int32_t>(W.ovf_a);
-      L.n_order = (int32_t)novf;
-      L.work_counter = &C->work[1];
-      L.ovf_list = P<int32_t>(W.ovf_b);
-      L.ovf_count = &C->ovf_count[1];
-      int blocks = ctx->sm_count * std::max(1, ctx->bps_large[pi]);
-      blocks = std::min<int>(blocks, (int)novf);
-      MV_CUDA(cudaEventRecord(ctx->ev[3], st));
-      MV_CUDA(launch_cells(L, true, blocks, st));
-      MV_CUDA(cudaEventRecord(ctx->ev[4], st));
-      launches++;
-      large_ran = true;
-      MV_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-      MV_CUDA(cudaStreamSynchronize(st));
+    {
+      const int rcp = run_cell_phase(ctx, J, JobTable{nullptr, nullptr, 0}, s.dim, o, n, pi, staged,
+                                     exporting, st, &launches, &stats, &hc);
+      if (rcp) return rcp;
     }
-    ctx->large_ran = large_ran;
     if (hc.status[STATUS_CODE]) {
       std::memset(out, 0, sizeof(*out));
       out->n_cells = n;
@@ -859,6 +900,349 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
   out->face_shift_code = P<uint8_t>(W.f_code);
   out->cell_face_connections = o.face_mode == MV_FACES_OWNED ? P<int32_t>(W.conn) : nullptr;
   out->error_cell = -1;
+  return MV_OK;
+}
+
+// ---- batches (mv_context_build_batch[_device]) ----
+// Builds many tessellations at once: per-tessellation setups on the host, one batch
+// grid (every tessellation's grid plus an empty end cell, one radix sort), the cell
+// phase over all cells with the job table, one finalize whose faces and CSR are then
+// made local to each tessellation.
+int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mask,
+                            const mv_job* jobs, int64_t njobs, const mv_options* opts_in,
+                            mv_batch_voronoi* out) {
+  mv_options o;
+  mv_options_default(&o);
+  if (opts_in) o = *opts_in;
+  if (!ctx || !out || !jobs || njobs <= 0 || njobs > (1 << 24)) return MV_ERR_ARG;
+  if (o.precision != MV_PRECISION_FP64 && o.precision != MV_PRECISION_FILTERED) return MV_ERR_ARG;
+  if (o.face_mode != MV_FACES_OWNED && o.face_mode != MV_FACES_ALL) return MV_ERR_ARG;
+  if (o.pipeline < MV_PIPELINE_AUTO || o.pipeline > MV_PIPELINE_FUSED || o.chunk_cells < 0)
+    return MV_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->error_job = -1;
+  out->error_cell = -1;
+  const int nj = (int)njobs;
+  std::vector<Setup> S(nj);
+  std::vector<int32_t> pos(nj + 1), cb(nj + 1);
+  std::vector<BatchGrid> bg(nj);
+  int64_t ntot = 0, ctot = 0;
+  bool any_mask = false;
+  double ratio = 0.0;
+  for (int j = 0; j < nj; j++) {
+    const mv_job& jb = jobs[j];
+    if (jb.n < 0 || jb.n >= (int64_t)(0xffffffffu / 27u)) return MV_ERR_ARG;
+    int rc = make_setup(jb.n, jb.anchor, jb.width, jb.dimensionality, jb.periodic, o, &S[j]);
+    if (rc) return rc;
+    pos[j] = (int32_t)ntot;
+    cb[j] = (int32_t)ctot;
+    ntot += jb.n;
+    ctot += (int64_t)S[j].G[0] * S[j].G[1] * S[j].G[2] + 1;
+    if (ntot >= INT32_MAX || ctot >= INT32_MAX) return MV_ERR_ARG;
+    BatchGrid& g = bg[j];
+    std::memset(&g, 0, sizeof(g));
+    for (int i = 0; i < 3; i++) g.G[i] = S[j].G[i], g.a[i] = S[j].anchor[i], g.inv[i] = S[j].ginv[i];
+    g.dim = S[j].dim;
+    g.cbase = cb[j];
+    any_mask |= jb.has_mask != 0;
+    ratio = std::max(ratio, face_ratio(S[j].dim, o.face_mode));
+  }
+  pos[nj] = (int32_t)ntot;
+  cb[nj] = (int32_t)ctot;
+  if ((ntot > 0 && !d_xyz) || (any_mask && !d_mask)) return MV_ERR_ARG;
+  MV_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  Workspace& W = ctx->ws;
+  const int ni = (int)ntot;
+  const size_t N = (size_t)std::max<int64_t>(ntot, 1);
+  const int64_t ncell = ctot;
+
+  // ---- workspace ----
+  int e = 0;
+  e |= ensure(ctx, W.gen, 24 * N);
+  e |= ensure(ctx, W.sx, 8 * N);
+  e |= ensure(ctx, W.sy, 8 * N);
+  e |= ensure(ctx, W.sz, 8 * N);
+  e |= ensure(ctx, W.sid, 4 * N);
+  e |= ensure(ctx, W.cid, 4 * N);
+  e |= ensure(ctx, W.cell_count, 4 * (ncell + 1));
+  e |= ensure(ctx, W.cell_start, 4 * (ncell + 1));
+  e |= ensure(ctx, W.dflag, 4 * (ncell + 1));
+  e |= ensure(ctx, W.dprefix, 4 * (ncell + 1));
+  e |= ensure(ctx, W.scan_tmp, 8 * (scan_tmp_elems(std::max<int64_t>(ncell + 1, N)) + 64));
+  e |= ensure(ctx, W.volume, 8 * N);
+  e |= ensure(ctx, W.centroid, 24 * N);
+  e |= ensure(ctx, W.sr, 8 * N);
+  e |= ensure(ctx, W.face_count, 4 * N);
+  e |= ensure(ctx, W.stage_off, 8 * N);
+  e |= ensure(ctx, W.face_off, 8 * (N + 1));
+  e |= ensure(ctx, W.in_count, 4 * N);
+  e |= ensure(ctx, W.conn_count, 4 * N);
+  e |= ensure(ctx, W.conn_off, 8 * (N + 1));
+  e |= ensure(ctx, W.cursor, 4 * N);
+  e |= ensure(ctx, W.ovf_a, 4 * N);
+  e |= ensure(ctx, W.ovf_b, 4 * N);
+  e |= ensure(ctx, W.counters, sizeof(DevCounters));
+  e |= ensure(ctx, W.dkey_a, 8 * N);
+  e |= ensure(ctx, W.dkey_b, 8 * N);
+  e |= ensure(ctx, W.dval_a, 4 * N);
+  e |= ensure(ctx, W.dval_b, 4 * N);
+  e |= ensure(ctx, W.fkey, 4 * N);
+  const size_t sort_bytes = grid_dense_sort_bytes(ni, ncell);
+  e |= ensure(ctx, W.dsort_tmp, sort_bytes + 256);
+  e |= ensure(ctx, W.b_jobs, sizeof(Job) * (size_t)nj);
+  e |= ensure(ctx, W.b_pos, 4 * (size_t)(nj + 1));
+  e |= ensure(ctx, W.b_cbase, 4 * (size_t)(nj + 1));
+  e |= ensure(ctx, W.b_grid, sizeof(BatchGrid) * (size_t)nj);
+  e |= ensure(ctx, W.b_ext_keys, 8 * 6 * (size_t)nj);
+  e |= ensure(ctx, W.b_ext, 8 * 6 * (size_t)nj);
+  e |= ensure(ctx, W.b_fbase, 8 * (size_t)(nj + 1));
+  e |= ensure(ctx, W.b_cbconn, 8 * (size_t)(nj + 1));
+  if (e) return MV_ERR_OOM;
+  const int32_t* d_pos = P<int32_t>(W.b_pos);
+  MV_CUDA(cudaMemcpyAsync(W.b_pos.p, pos.data(), 4 * (size_t)(nj + 1), cudaMemcpyHostToDevice, st));
+  MV_CUDA(cudaMemcpyAsync(W.b_cbase.p, cb.data(), 4 * (size_t)(nj + 1), cudaMemcpyHostToDevice, st));
+  MV_CUDA(cudaMemcpyAsync(W.b_grid.p, bg.data(), sizeof(BatchGrid) * (size_t)nj, cudaMemcpyHostToDevice, st));
+  const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
+  {
+    const size_t bb = cells_big_bytes(ctx->sm_count * std::max(1, ctx->bps_fast[pi]),
+                                      ctx->sm_count * std::max(1, ctx->bps_large[pi]));
+    if (ensure(ctx, W.big, bb)) return MV_ERR_OOM;
+  }
+  ratio = std::max(ratio, ctx->face_ratio_hint);
+  int64_t face_cap = (int64_t)(ratio * (double)ntot) + 4096;
+
+  DevCounters* C = P<DevCounters>(W.counters);
+  mv_build_stats stats{};
+  int64_t launches = 0;
+  int64_t F = 0;
+  std::vector<Job> JJ(nj);
+  for (int attempt = 0;; attempt++) {
+    size_t FC = (size_t)face_cap;
+    e = 0;
+    e |= ensure(ctx, W.st_left, 4 * FC);
+    e |= ensure(ctx, W.st_right, 4 * FC);
+    e |= ensure(ctx, W.st_area, 8 * FC);
+    e |= ensure(ctx, W.st_cen, 24 * FC);
+    e |= ensure(ctx, W.st_nrm, 24 * FC);
+    e |= ensure(ctx, W.st_code, FC);
+    if (e) return MV_ERR_OOM;
+    face_cap = (int64_t)std::min(W.st_left.cap / 4, W.st_code.cap);
+    face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_area.cap / 8));
+    face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_cen.cap / 24));
+    MV_CUDA(cudaMemsetAsync(C, 0, sizeof(DevCounters), st));
+    MV_CUDA(cudaMemsetAsync(W.cell_count.p, 0, 4 * (ncell + 1), st));
+
+    // ---- generators + batch grid ----
+    MV_CUDA(cudaEventRecord(ctx->ev[0], st));
+    launch_batch_grid(d_xyz, ni, d_pos, P<int32_t>(W.b_cbase), nj, P<BatchGrid>(W.b_grid), ncell,
+                      P<double>(W.gen), P<unsigned long long>(W.b_ext_keys), P<double>(W.b_ext),
+                      &C->bad_input, P<int32_t>(W.cid), P<int32_t>(W.cell_count),
+                      P<int32_t>(W.cell_start), P<int32_t>(W.dflag), P<int32_t>(W.dprefix),
+                      P<long long>(W.scan_tmp), st);
+    MV_CUDA(launch_batch_sort(P<double>(W.gen), ni, d_pos, P<int32_t>(W.b_cbase), nj, P<BatchGrid>(W.b_grid),
+                              ncell, P<int32_t>(W.cid), P<int32_t>(W.dflag), P<unsigned long long>(W.dkey_a),
+                              P<unsigned long long>(W.dkey_b), P<int32_t>(W.dval_a), P<int32_t>(W.dval_b),
+                              W.dsort_tmp.p, W.dsort_tmp.cap, P<double>(W.sx), P<double>(W.sy),
+                              P<double>(W.sz), P<int32_t>(W.sid), P<uint32_t>(W.fkey),
+                              P<int32_t>(W.cell_start), st));
+    launches += 19;  // ext init/prep/finish, cell index, 2 x 3 scan kernels, dense flags, keys, sort, gather, starts
+
+    // ---- one Job per tessellation, addressing its slices ----
+    for (int j = 0; j < nj; j++) {
+      const Setup& sj = S[j];
+      Job& J = JJ[j];
+      std::memset(&J, 0, sizeof(J));
+      const int64_t pb = pos[j], cbj = cb[j];
+      J.gen = P<double>(W.gen) + 3 * pb;
+      J.sx = P<double>(W.sx) + pb;
+      J.sy = P<double>(W.sy) + pb;
+      J.sz = P<double>(W.sz) + pb;
+      J.sid = P<int32_t>(W.sid) + pb;
+      J.cell_start = P<int32_t>(W.cell_start) + cbj;
+      J.dprefix = P<int32_t>(W.dprefix) + cbj;
+      J.cell_dense = P<int32_t>(W.dflag) + cbj;
+      J.fkey = P<uint32_t>(W.fkey) + pb;
+      J.fbits = fkey_bits(sj.dim);
+      J.mask = jobs[j].has_mask ? d_mask + pb : nullptr;
+      J.n = (int32_t)jobs[j].n;
+      J.dim = sj.dim;
+      J.periodic = sj.periodic;
+      J.face_mode = o.face_mode;
+      J.precision = o.precision;
+      for (int i = 0; i < 3; i++) {
+        J.G[i] = sj.G[i];
+        J.ga[i] = sj.anchor[i];
+        J.gw[i] = sj.width[i];
+        J.gh[i] = sj.gh[i];
+        J.ginv[i] = sj.ginv[i];
+        J.geps[i] = sj.geps[i];
+        J.iloc_a[i] = sj.iloc_a[i];
+        J.iloc_inv[i] = sj.iloc_inv[i];
+      }
+      J.ext = P<double>(W.b_ext) + 6 * j;
+      J.R0 = sj.R0;
+      J.ppc_mean = (double)std::max<int64_t>(jobs[j].n, 1) / (double)(cb[j + 1] - cb[j] - 1);
+      for (int c = 0; c < 27; c++) {
+        const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
+        for (int i = 0; i < 3; i++) {
+          const double q = (double)(-m[i]) * sj.width[i];
+          J.qshift[c][i] = q;
+          J.shift[c][i] = -q;
+        }
+      }
+      for (int k = 0; k < 6; k++) {
+        for (int i = 0; i < 3; i++) J.bn[k][i] = sj.bn[k][i], J.bp[k][i] = sj.bp[k][i];
+        J.bd[k] = sj.bd[k];
+      }
+      J.volume = P<double>(W.volume) + pb;
+      J.centroid = P<double>(W.centroid) + 3 * pb;
+      J.safety_radius = P<double>(W.sr) + pb;
+      J.face_count = P<int32_t>(W.face_count) + pb;
+      J.stage_off = P<int64_t>(W.stage_off) + pb;
+      J.f_left = P<int32_t>(W.st_left);
+      J.f_right = P<int32_t>(W.st_right);
+      J.f_area = P<double>(W.st_area);
+      J.f_centroid = P<double>(W.st_cen);
+      J.f_normal = P<double>(W.st_nrm);
+      J.f_code = P<uint8_t>(W.st_code);
+      J.face_counter = &C->face_counter;
+      J.face_cap = face_cap;
+      J.work_counter = &C->work[0];
+      J.ovf_list = P<int32_t>(W.ovf_a);
+      J.ovf_count = &C->ovf_count[0];
+      J.status = C->status;
+      J.stats = C->stats;
+      J.big = static_cast<char*>(W.big.p);
+      J.id_base = (int32_t)pb;
+    }
+    MV_CUDA(cudaMemcpyAsync(W.b_jobs.p, JJ.data(), sizeof(Job) * (size_t)nj, cudaMemcpyHostToDevice, st));
+    // the template Job: shared fields (counters, staging, queues) and the batch's size
+    Job J0 = JJ[0];
+    J0.n = ni;
+    J0.order = nullptr;
+    J0.n_order = ni;
+    const JobTable TB{P<Job>(W.b_jobs), d_pos, nj};
+    DevCounters hc;
+    {
+      const int rcp = run_cell_phase(ctx, J0, TB, 3, o, ntot, pi, true, false, st, &launches, &stats, &hc);
+      if (rcp) return rcp;
+    }
+    if (hc.status[STATUS_CODE]) {
+      const int64_t g = hc.status[STATUS_CELL];
+      const int jf = (int)(std::upper_bound(pos.begin(), pos.end() - 1, (int32_t)g) - pos.begin()) - 1;
+      out->n_jobs = nj;
+      out->error_job = jf;
+      out->error_cell = g - pos[std::max(jf, 0)];
+      return hc.status[STATUS_CODE];
+    }
+    if (hc.ovf_count[1] > 0) return MV_ERR_CAPACITY;
+    if (hc.status[STATUS_REC_OVERFLOW]) {
+      if (attempt >= 2) return MV_ERR_CAPACITY;
+      ctx->rec_words_hint = 1.2 * (double)hc.rec_counter / (double)std::max<int64_t>(ntot, 1) + 8.0;
+      continue;
+    }
+    if (hc.status[STATUS_FACE_OVERFLOW]) {
+      if (attempt >= 2) return MV_ERR_CAPACITY;
+      face_cap = (int64_t)(hc.face_counter * 1.15) + 4096;
+      ctx->face_ratio_hint = (double)face_cap / (double)std::max<int64_t>(ntot, 1);
+      continue;
+    }
+    F = (int64_t)hc.face_counter;
+    stats.cells_built = (int64_t)hc.stats[ST_CELLS];
+    stats.neighbours_clipped = (int64_t)hc.stats[ST_NEIGHBOURS];
+    stats.planes_added = (int64_t)hc.stats[ST_PLANES];
+    stats.f32_undecided = (int64_t)hc.stats[ST_F32_UNDECIDED];
+    stats.exact_tests = (int64_t)hc.stats[ST_EXACT];
+    stats.extra_shells = (int64_t)hc.stats[ST_SHELLS];
+    stats.overflow_cells = (int64_t)hc.stats[ST_OVERFLOW];
+    stats.serial_rings = (int64_t)hc.stats[ST_SERIAL_RING];
+    break;
+  }
+
+  // ---- flatten + finalize over the batch, then local indices ----
+  {
+    size_t FF = (size_t)std::max<int64_t>(F, 1);
+    e = 0;
+    e |= ensure(ctx, W.f_left, 4 * FF);
+    e |= ensure(ctx, W.f_right, 4 * FF);
+    e |= ensure(ctx, W.f_area, 8 * FF);
+    e |= ensure(ctx, W.f_cen, 24 * FF);
+    e |= ensure(ctx, W.f_nrm, 24 * FF);
+    e |= ensure(ctx, W.f_code, FF);
+    if (e) return MV_ERR_OOM;
+  }
+  MV_CUDA(cudaEventRecord(ctx->ev[5], st));
+  scan_i32_to_i64(P<int32_t>(W.face_count), ntot, P<int64_t>(W.face_off), P<long long>(W.scan_tmp), st);
+  FaceArrays stage{P<int32_t>(W.st_left), P<int32_t>(W.st_right), P<double>(W.st_area),
+                   P<double>(W.st_cen), P<double>(W.st_nrm), P<uint8_t>(W.st_code)};
+  FaceArrays fin{P<int32_t>(W.f_left), P<int32_t>(W.f_right), P<double>(W.f_area),
+                 P<double>(W.f_cen), P<double>(W.f_nrm), P<uint8_t>(W.f_code)};
+  launch_reorder(stage, F, P<int64_t>(W.stage_off), P<int64_t>(W.face_off), fin, st);
+  launches += 4;
+  int64_t Cn = 0;
+  const bool owned = o.face_mode == MV_FACES_OWNED;
+  if (owned) {
+    MV_CUDA(cudaMemsetAsync(W.in_count.p, 0, 4 * N, st));
+    MV_CUDA(cudaMemsetAsync(W.cursor.p, 0, 4 * N, st));
+    launch_batch_csr(fin, F, P<int64_t>(W.face_off), P<int32_t>(W.face_count), ni, d_pos, nj,
+                     P<int32_t>(W.in_count), P<int32_t>(W.conn_count), st);
+    scan_i32_to_i64(P<int32_t>(W.conn_count), ntot, P<int64_t>(W.conn_off), P<long long>(W.scan_tmp), st);
+    MV_CUDA(cudaMemcpyAsync(&Cn, P<int64_t>(W.conn_off) + ntot, 8, cudaMemcpyDeviceToHost, st));
+    MV_CUDA(cudaStreamSynchronize(st));
+    if (ensure(ctx, W.conn, 4 * (size_t)std::max<int64_t>(Cn, 1))) return MV_ERR_OOM;
+    launch_batch_csr_fill(fin, F, P<int64_t>(W.face_off), P<int64_t>(W.conn_off), P<int32_t>(W.in_count),
+                          P<int32_t>(W.cursor), ni, d_pos, nj, P<int32_t>(W.conn), st);
+    launches += 7;
+  }
+  launch_batch_localize(fin, F, P<int64_t>(W.face_off), owned ? P<int64_t>(W.conn_off) : nullptr,
+                        P<int32_t>(W.conn_count), P<int32_t>(W.conn), ni, d_pos, nj, P<int64_t>(W.b_fbase),
+                        P<int64_t>(W.b_cbconn), st);
+  launches += owned ? 3 : 2;
+  MV_CUDA(cudaEventRecord(ctx->ev[6], st));
+  ctx->bj_cell.assign(pos.begin(), pos.end());
+  ctx->bj_face.assign(nj + 1, 0);
+  ctx->bj_conn.assign(nj + 1, 0);
+  MV_CUDA(cudaMemcpyAsync(ctx->bj_face.data(), W.b_fbase.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost, st));
+  if (owned)
+    MV_CUDA(cudaMemcpyAsync(ctx->bj_conn.data(), W.b_cbconn.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost,
+                            st));
+  MV_CUDA(cudaGetLastError());
+  MV_CUDA(cudaStreamSynchronize(st));
+  stats.device_bytes = (int64_t)ctx->dev_bytes;
+  stats.kernel_launches = launches;
+  {
+    float t01 = 0.f, t12 = 0.f, t34 = 0.f, t56 = 0.f, t78 = 0.f;
+    cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&t12, ctx->ev[1], ctx->ev[2]);
+    if (ctx->large_ran) cudaEventElapsedTime(&t34, ctx->ev[3], ctx->ev[4]);
+    if (ctx->retry_ran) cudaEventElapsedTime(&t78, ctx->ev[7], ctx->ev[8]);
+    cudaEventElapsedTime(&t56, ctx->ev[5], ctx->ev[6]);
+    stats.ms_grid = t01;
+    stats.ms_cells = t12 + t34 + t78;
+    stats.ms_retry = t78;
+    stats.ms_finalize = t56;
+  }
+  ctx->last = stats;
+  out->n_jobs = nj;
+  out->n_cells = ntot;
+  out->n_faces = F;
+  out->n_connections = Cn;
+  out->job_cell_offset = ctx->bj_cell.data();
+  out->job_face_offset = ctx->bj_face.data();
+  out->job_connection_offset = ctx->bj_conn.data();
+  out->cell_volume = P<double>(W.volume);
+  out->cell_centroid = P<double>(W.centroid);
+  out->cell_safety_radius = P<double>(W.sr);
+  out->cell_face_offset = owned ? P<int64_t>(W.conn_off) : nullptr;
+  out->cell_face_count = owned ? P<int32_t>(W.conn_count) : nullptr;
+  out->face_left = P<int32_t>(W.f_left);
+  out->face_right = P<int32_t>(W.f_right);
+  out->face_area = P<double>(W.f_area);
+  out->face_centroid = P<double>(W.f_cen);
+  out->face_normal = P<double>(W.f_nrm);
+  out->face_shift_code = P<uint8_t>(W.f_code);
+  out->cell_face_connections = owned ? P<int32_t>(W.conn) : nullptr;
   return MV_OK;
 }
 
@@ -1037,6 +1421,85 @@ int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int
     if (rc) return rc;
     *cells_out = &ctx->hc;
   }
+  return MV_OK;
+}
+
+// Batch build with host inputs: inputs copied to the device, the result copied into the
+// context's pinned host arena (same layout as a single build's).
+int build_batch_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, const mv_job* jobs,
+                          int64_t njobs, const mv_options* opts, mv_batch_voronoi* out) {
+  if (!ctx || !out || !jobs || njobs <= 0) return MV_ERR_ARG;
+  mv_options o;
+  mv_options_default(&o);
+  if (opts) o = *opts;
+  int64_t ntot = 0;
+  bool any_mask = false;
+  for (int64_t j = 0; j < njobs; j++) {
+    if (jobs[j].n < 0) return MV_ERR_ARG;
+    ntot += jobs[j].n;
+    any_mask |= jobs[j].has_mask != 0;
+  }
+  if ((ntot > 0 && !xyz) || (any_mask && !mask)) return MV_ERR_ARG;
+  MV_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  const size_t N = (size_t)std::max<int64_t>(ntot, 1);
+  if (ensure(ctx, ctx->ws.in_xyz, 24 * N) || ensure(ctx, ctx->ws.in_mask, N)) return MV_ERR_OOM;
+  if (ntot > 0)
+    MV_CUDA(cudaMemcpyAsync(ctx->ws.in_xyz.p, xyz, 24 * (size_t)ntot, cudaMemcpyHostToDevice, st));
+  if (any_mask && ntot > 0)
+    MV_CUDA(cudaMemcpyAsync(ctx->ws.in_mask.p, mask, (size_t)ntot, cudaMemcpyHostToDevice, st));
+  mv_batch_voronoi d;
+  int rc = build_batch_device_impl(ctx, P<double>(ctx->ws.in_xyz), any_mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr,
+                                   jobs, njobs, &o, &d);
+  if (rc) {
+    *out = d;
+    return rc;
+  }
+  HostLayout L = host_layout(d.n_cells, d.n_faces, d.n_connections);
+  if (ctx->host_cap < L.total) {
+    if (ctx->host) cudaFreeHost(ctx->host);
+    ctx->host = nullptr;
+    ctx->host_cap = 0;
+    const size_t want = L.total + L.total / 8 + 4096;
+    if (cudaHostAlloc(&ctx->host, want, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->host = nullptr;
+      return MV_ERR_OOM;
+    }
+    ctx->host_cap = want;
+  }
+  char* b = static_cast<char*>(ctx->host);
+  *out = d;
+  out->cell_volume = (double*)(b + L.off[0]);
+  out->cell_centroid = (double*)(b + L.off[1]);
+  out->cell_safety_radius = (double*)(b + L.off[2]);
+  out->cell_face_offset = d.cell_face_offset ? (int64_t*)(b + L.off[3]) : nullptr;
+  out->cell_face_count = d.cell_face_count ? (int32_t*)(b + L.off[4]) : nullptr;
+  out->face_left = (int32_t*)(b + L.off[5]);
+  out->face_right = (int32_t*)(b + L.off[6]);
+  out->face_area = (double*)(b + L.off[7]);
+  out->face_centroid = (double*)(b + L.off[8]);
+  out->face_normal = (double*)(b + L.off[9]);
+  out->face_shift_code = (uint8_t*)(b + L.off[10]);
+  out->cell_face_connections = d.cell_face_connections ? (int32_t*)(b + L.off[11]) : nullptr;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    if (!bytes || !src || !dst) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  const size_t n = (size_t)d.n_cells, F = (size_t)d.n_faces, Cn = (size_t)d.n_connections;
+  MV_CUDA(cp(out->cell_volume, d.cell_volume, 8 * n));
+  MV_CUDA(cp(out->cell_centroid, d.cell_centroid, 24 * n));
+  MV_CUDA(cp(out->cell_safety_radius, d.cell_safety_radius, 8 * n));
+  MV_CUDA(cp(out->cell_face_offset, d.cell_face_offset, 8 * n));
+  MV_CUDA(cp(out->cell_face_count, d.cell_face_count, 4 * n));
+  MV_CUDA(cp(out->face_left, d.face_left, 4 * F));
+  MV_CUDA(cp(out->face_right, d.face_right, 4 * F));
+  MV_CUDA(cp(out->face_area, d.face_area, 8 * F));
+  MV_CUDA(cp(out->face_centroid, d.face_centroid, 24 * F));
+  MV_CUDA(cp(out->face_normal, d.face_normal, 24 * F));
+  MV_CUDA(cp(out->face_shift_code, d.face_shift_code, F));
+  MV_CUDA(cp(out->cell_face_connections, d.cell_face_connections, 4 * Cn));
+  MV_CUDA(cudaStreamSynchronize(st));
   return MV_OK;
 }
 
@@ -1233,6 +1696,18 @@ int mv_voronoi_build_partial(const double* generators, const uint8_t* mask, int6
                              int periodic, const mv_options* opts, mv_voronoi** out) {
   if (!anchor || !width || (n > 0 && !mask)) return MV_ERR_ARG;
   return standalone(generators, mask, n, anchor, width, dimensionality, periodic, opts, out);
+}
+
+int mv_context_build_batch_device(mv_context* ctx, const double* d_generators, const uint8_t* d_mask,
+                                  const mv_job* jobs, int64_t n_jobs, const mv_options* opts,
+                                  mv_batch_voronoi* out) {
+  return build_batch_device_impl(ctx, d_generators, d_mask, jobs, n_jobs, opts, out);
+}
+
+int mv_context_build_batch(mv_context* ctx, const double* generators, const uint8_t* mask,
+                           const mv_job* jobs, int64_t n_jobs, const mv_options* opts,
+                           mv_batch_voronoi* out) {
+  return build_batch_host_impl(ctx, generators, mask, jobs, n_jobs, opts, out);
 }
 
 void mv_voronoi_free(mv_voronoi* v) {

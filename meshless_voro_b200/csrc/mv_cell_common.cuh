@@ -423,6 +423,19 @@ __device__ __forceinline__ int big_stop(const Job& J) {
   return J.big != nullptr ? BIG_CAP : 32 * CMAX;
 }
 
+// Tessellation of batch position pos (the last j with pos_base[j] <= pos).
+__device__ __forceinline__ int job_of(const JobTable& T, int pos) {
+  int a = 0, b = T.njobs - 1;
+  while (a < b) {
+    const int m = (a + b + 1) >> 1;
+    if (__ldg(T.pos_base + m) <= pos)
+      a = m;
+    else
+      b = m - 1;
+  }
+  return a;
+}
+
 // Gathers every stream element (generator, periodic image) with lo2 <= d2 < R*R into
 // B (unsorted) and returns how many there are (may exceed CMAX; once the count passes
 // stop the gather ends early and returns a count above stop).  With BIG and a slot,
@@ -1231,7 +1244,7 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
       const int64_t f = (int64_t)base + rank_base + __popc(bal & lanemask_lt());
       const double na = fa[k] > 0.0 ? 1.0 / (3.0 * fa[k]) : 0.0;
       const D3 nn = V.normal(pl);
-      J.f_left[f] = self;
+      J.f_left[f] = self + J.id_base;
       J.f_right[f] = V.right(pl);
       J.f_area[f] = fa[k];
       J.f_centroid[3 * f] = fcx[k] * na;

@@ -459,22 +459,28 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   return res;
 }
 
-template <class T, int PREC, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid_constant__ Job J) {
+template <class T, int PREC, int WARPS, bool MULTI>
+__global__ void __launch_bounds__(32 * WARPS, T::MINB)
+    cells_kernel(const __grid_constant__ Job J0, const __grid_constant__ JobTable TB) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   CellSmem<T>& S = reinterpret_cast<CellSmem<T>*>(smem_raw)[warp];
   __shared__ double ext_s[6];
-  if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  if (threadIdx.x < 6) ext_s[threadIdx.x] = J0.ext[threadIdx.x];
   if (lane < ST_COUNT) S.cnt[lane] = 0ull;
   __syncthreads();
-  const int total = J.order ? J.n_order : J.n;
+  const int total = J0.order ? J0.n_order : J0.n;
   for (;;) {
     int item = 0;
-    if (lane == 0) item = (int)atomicAdd(J.work_counter, 1u);
+    if (lane == 0) item = (int)atomicAdd(J0.work_counter, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= total) break;
-    const int spos = J.order ? J.order[item] : item;
+    const int gpos = J0.order ? J0.order[item] : item;
+    // the cell's tessellation (batch builds): its Job and its local position
+    const int jb = MULTI ? job_of(TB, gpos) : 0;
+    const Job& J = MULTI ? TB.jobs[jb] : J0;
+    const int spos = MULTI ? gpos - __ldg(TB.pos_base + jb) : gpos;
+    const double* ext = MULTI ? J.ext : ext_s;
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       // VoronoiCell::default() (voronoi.rs:303-305)
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
     CellCount cc;
 #pragma unroll
     for (int i = 0; i < ST_COUNT; i++) cc.c[i] = 0u;
-    const int res = build_cell<T, PREC>(J, S, lane, spos, ext_s, &err, cc);
+    const int res = build_cell<T, PREC>(J, S, lane, spos, ext, &err, cc);
     __syncwarp();
     if (res == CELL_DONE) cc.c[ST_CELLS]++;
     if (lane == 0) {
@@ -501,8 +507,8 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
     __syncwarp();
     if (res == CELL_OVERFLOW) {
       if (lane == 0) {
-        unsigned k = atomicAdd(J.ovf_count, 1u);
-        J.ovf_list[k] = spos;
+        unsigned k = atomicAdd(J0.ovf_count, 1u);
+        J0.ovf_list[k] = gpos;
         S.cnt[ST_OVERFLOW]++;
       }
     } else if (res == CELL_FACE_OVERFLOW) {
@@ -512,13 +518,13 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) cells_kernel(const __grid
     } else if (res == CELL_ERROR) {
       if (lane == 0) {
         atomicCAS(J.status + STATUS_CODE, 0, err);
-        atomicMin(J.status + STATUS_CELL, self);
+        atomicMin(J.status + STATUS_CELL, self + J.id_base);
       }
     }
     __syncwarp();
   }
   __syncwarp();
-  if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J.stats + lane, S.cnt[lane]);
+  if (lane < ST_COUNT && S.cnt[lane]) atomicAdd(J0.stats + lane, S.cnt[lane]);
 }
 
 // ---------------------------------------------------------------- launchers --
@@ -532,7 +538,7 @@ template <class T, int PREC, int WARPS>
 static int blocks_per_sm() {
   int nb = 0;
   const size_t smem = sizeof(CellSmem<T>) * WARPS;
-  auto k = cells_kernel<T, PREC, WARPS>;
+  auto k = cells_kernel<T, PREC, WARPS, false>;
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * WARPS, smem) != cudaSuccess) return 0;
@@ -540,12 +546,12 @@ static int blocks_per_sm() {
 }
 
 template <class T, int PREC, int WARPS>
-static cudaError_t launch_tier(const Job& J, int blocks, cudaStream_t st) {
+static cudaError_t launch_tier(const Job& J, const JobTable& TB, int blocks, cudaStream_t st) {
   const size_t smem = sizeof(CellSmem<T>) * WARPS;
-  auto k = cells_kernel<T, PREC, WARPS>;
+  auto k = TB.jobs != nullptr ? cells_kernel<T, PREC, WARPS, true> : cells_kernel<T, PREC, WARPS, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k<<<blocks, 32 * WARPS, smem, st>>>(J);
+  k<<<blocks, 32 * WARPS, smem, st>>>(J, TB);
   return cudaGetLastError();
 }
 
@@ -568,15 +574,17 @@ size_t cells_big_bytes(int blocks_fast, int blocks_large) {
   return warps * BIG_SLOT_BYTES;
 }
 
-cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st) {
+// The fused kernel over J's cells (J.order / J.n); with a job table (TB.jobs != nullptr)
+// over the cells of a batch.
+cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st, const JobTable& TB) {
   if (!large) {
     if (J.precision == MV_PRECISION_FILTERED)
-      return launch_tier<TierFast, MV_PRECISION_FILTERED, FAST_WARPS>(J, blocks, st);
-    return launch_tier<TierFast, MV_PRECISION_FP64, FAST_WARPS>(J, blocks, st);
+      return launch_tier<TierFast, MV_PRECISION_FILTERED, FAST_WARPS>(J, TB, blocks, st);
+    return launch_tier<TierFast, MV_PRECISION_FP64, FAST_WARPS>(J, TB, blocks, st);
   }
   if (J.precision == MV_PRECISION_FILTERED)
-    return launch_tier<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>(J, blocks, st);
-  return launch_tier<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>(J, blocks, st);
+    return launch_tier<TierLarge, MV_PRECISION_FILTERED, LARGE_WARPS>(J, TB, blocks, st);
+  return launch_tier<TierLarge, MV_PRECISION_FP64, LARGE_WARPS>(J, TB, blocks, st);
 }
 
 }  // namespace mv

@@ -302,6 +302,204 @@ __global__ void conn_sort_kernel(const int64_t* __restrict__ conn_off,
   }
 }
 
+// ------------------------------------------------------------------ batches --
+// A batch concatenates its tessellations: tessellation j owns the input indices and
+// sorted positions [pos[j], pos[j + 1]) and the grid cells [cbase[j], cbase[j + 1])
+// (its own grid plus one empty end cell, so that its cell_start slice ends with its
+// own end).  The kernels below find a point's, cell's or face's tessellation by binary
+// search over these bases.
+__device__ __forceinline__ int batch_find(const int32_t* __restrict__ base, int nj, int64_t v) {
+  int a = 0, b = nj - 1;
+  while (a < b) {
+    const int m = (a + b + 1) >> 1;
+    if (base[m] <= v)
+      a = m;
+    else
+      b = m - 1;
+  }
+  return a;
+}
+
+__global__ void batch_ext_init_kernel(unsigned long long* ext_keys, int nj) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 6 * nj) ext_keys[i] = (i % 6) < 3 ? ~0ull : 0ull;
+}
+
+// Generator::new per tessellation (its dimensionality) and each tessellation's extent;
+// a warp whose points all belong to one tessellation reduces before its atomics.
+__global__ void batch_prep_kernel(const double* __restrict__ xyz, int n, const int32_t* __restrict__ pos,
+                                  int nj, const BatchGrid* __restrict__ bg, double* __restrict__ gen,
+                                  unsigned long long* ext_keys, int* bad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int j = -1;
+  unsigned long long kmin[3] = {~0ull, ~0ull, ~0ull}, kmax[3] = {0ull, 0ull, 0ull};
+  if (k < n) {
+    j = batch_find(pos, nj, k);
+    const int dim = bg[j].dim;
+    double c[3] = {xyz[3 * (int64_t)k], xyz[3 * (int64_t)k + 1], xyz[3 * (int64_t)k + 2]};
+    if (dim == 1) c[1] = 0.0, c[2] = 0.0;
+    if (dim == 2) c[2] = 0.0;
+    bool fin = true;
+    for (int i = 0; i < 3; i++) {
+      gen[3 * (int64_t)k + i] = c[i];
+      fin &= isfinite(c[i]);
+      kmin[i] = kmax[i] = ord_key(c[i]);
+    }
+    if (!fin) atomicExch(bad, 1);
+  }
+  const int j0 = __shfl_sync(0xffffffffu, j, 0);
+  if (__all_sync(0xffffffffu, j == j0) && j0 >= 0) {
+    for (int o = 16; o > 0; o >>= 1)
+      for (int i = 0; i < 3; i++) {
+        kmin[i] = min(kmin[i], __shfl_xor_sync(0xffffffffu, kmin[i], o));
+        kmax[i] = max(kmax[i], __shfl_xor_sync(0xffffffffu, kmax[i], o));
+      }
+    if (lane == 0)
+      for (int i = 0; i < 3; i++) {
+        atomicMin(&ext_keys[6 * j0 + i], kmin[i]);
+        atomicMax(&ext_keys[6 * j0 + 3 + i], kmax[i]);
+      }
+  } else if (j >= 0) {
+    for (int i = 0; i < 3; i++) {
+      atomicMin(&ext_keys[6 * j + i], kmin[i]);
+      atomicMax(&ext_keys[6 * j + 3 + i], kmax[i]);
+    }
+  }
+}
+
+__global__ void batch_ext_finish_kernel(const unsigned long long* ext_keys, double* ext, int nj) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 6 * nj) ext[i] = ord_val(ext_keys[i]);
+}
+
+// grid cell (batch-wide index) of each generator, and the cell counts
+__global__ void batch_cell_index_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ pos,
+                                        int nj, const BatchGrid* __restrict__ bg, int32_t* __restrict__ cid,
+                                        int32_t* __restrict__ count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const BatchGrid& g = bg[batch_find(pos, nj, k)];
+  int c[3];
+  for (int i = 0; i < 3; i++) {
+    double f = floor((gen[3 * (int64_t)k + i] - g.a[i]) * g.inv[i]);
+    if (!(f >= 0.0)) f = 0.0;
+    if (f > g.G[i] - 1) f = g.G[i] - 1;
+    c[i] = (int)f;
+  }
+  const int id = g.cbase + c[0] + g.G[0] * (c[1] + g.G[1] * c[2]);
+  cid[k] = id;
+  atomicAdd(count + id, 1);
+}
+
+// sort key: batch cell << FKEY_BITS | Morton key inside a dense cell
+__global__ void batch_key_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ pos,
+                                 int nj, const BatchGrid* __restrict__ bg, const int32_t* __restrict__ cid,
+                                 const int32_t* __restrict__ dflag, unsigned long long* __restrict__ key,
+                                 int32_t* __restrict__ val) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = cid[k];
+  uint32_t m = 0;
+  if (dflag[c]) {
+    const BatchGrid& g = bg[batch_find(pos, nj, k)];
+    const int bits = fkey_bits(g.dim);
+    const int lc = c - g.cbase;
+    const int cc[3] = {lc % g.G[0], (lc / g.G[0]) % g.G[1], lc / (g.G[0] * g.G[1])};
+    uint32_t q[3] = {0u, 0u, 0u};
+    for (int i = 0; i < g.dim; i++) q[i] = fine_q(gen[3 * (int64_t)k + i], g.a[i], g.inv[i], cc[i], bits);
+    m = morton(g.dim, q[0], q[1], q[2]);
+  }
+  key[k] = ((unsigned long long)c << FKEY_BITS) | m;
+  val[k] = k;
+}
+
+// sorted position s <- generator val[s]; sid holds the tessellation-local index
+__global__ void batch_gather_kernel(const double* __restrict__ gen, int n,
+                                    const unsigned long long* __restrict__ key,
+                                    const int32_t* __restrict__ val, const int32_t* __restrict__ pos,
+                                    int nj, double* __restrict__ sx, double* __restrict__ sy,
+                                    double* __restrict__ sz, int32_t* __restrict__ sid,
+                                    uint32_t* __restrict__ fkey) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int k = val[s];
+  sx[s] = gen[3 * (int64_t)k];
+  sy[s] = gen[3 * (int64_t)k + 1];
+  sz[s] = gen[3 * (int64_t)k + 2];
+  sid[s] = k - pos[batch_find(pos, nj, k)];
+  fkey[s] = (uint32_t)(key[s] & ((1ull << FKEY_BITS) - 1ull));
+}
+
+// cell_start entries of tessellation j's cells (and end cell) become local positions
+__global__ void batch_local_starts_kernel(int32_t* __restrict__ start, int64_t ncell,
+                                          const int32_t* __restrict__ cbase, const int32_t* __restrict__ pos,
+                                          int nj) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  start[c] -= pos[batch_find(cbase, nj, c)];
+}
+
+// Voronoi::finalize over a batch: faces carry the batch position of their left cell
+// until the CSR is built; right indices are local to the tessellation
+__global__ void batch_in_count_kernel(const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+                                      const uint8_t* __restrict__ code, int64_t F,
+                                      const int32_t* __restrict__ pos, int nj, int32_t* __restrict__ in_count) {
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  const int r = right[f];
+  if (r >= 0 && code[f] == 13) atomicAdd(in_count + r + pos[batch_find(pos, nj, left[f])], 1);
+}
+
+__global__ void batch_conn_fill_kernel(const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+                                       const uint8_t* __restrict__ code, const int64_t* __restrict__ face_off,
+                                       const int64_t* __restrict__ conn_off,
+                                       const int32_t* __restrict__ in_count, int32_t* __restrict__ cursor,
+                                       int64_t F, const int32_t* __restrict__ pos, int nj,
+                                       int32_t* __restrict__ conn) {
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  const int l = left[f];
+  conn[conn_off[l] + in_count[l] + (f - face_off[l])] = (int32_t)f;
+  const int r = right[f];
+  if (r >= 0 && code[f] == 13) {
+    const int rg = r + pos[batch_find(pos, nj, l)];
+    const int slot = atomicAdd(cursor + rg, 1);
+    conn[conn_off[rg] + slot] = (int32_t)f;
+  }
+}
+
+// first face and first connection of each tessellation (j = nj: the totals)
+__global__ void batch_bases_kernel(const int64_t* __restrict__ face_off, const int64_t* __restrict__ conn_off,
+                                   const int32_t* __restrict__ pos, int nj, int64_t* __restrict__ fbase,
+                                   int64_t* __restrict__ cbase_conn) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > nj) return;
+  fbase[j] = face_off[pos[j]];
+  if (conn_off != nullptr) cbase_conn[j] = conn_off[pos[j]];
+}
+
+// faces: left becomes local; CSR: offsets and face indices become local
+__global__ void batch_local_faces_kernel(int32_t* __restrict__ left, int64_t F, const int32_t* __restrict__ pos,
+                                         int nj) {
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  left[f] -= pos[batch_find(pos, nj, left[f])];
+}
+
+__global__ void batch_local_conn_kernel(int64_t* __restrict__ conn_off, const int32_t* __restrict__ conn_count,
+                                        int32_t* __restrict__ conn, int n, const int32_t* __restrict__ pos,
+                                        int nj, const int64_t* __restrict__ fbase,
+                                        const int64_t* __restrict__ cbase_conn) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int j = batch_find(pos, nj, c);
+  const int64_t o = conn_off[c];
+  const int32_t fb = (int32_t)fbase[j];
+  for (int i = 0; i < conn_count[c]; i++) conn[o + i] -= fb;
+  conn_off[c] = o - cbase_conn[j];
+}
+
 // ---------------------------------------------------------------- launchers --
 static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
@@ -419,6 +617,66 @@ void launch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, co
     conn_fill_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, F, face_off, conn_off,
                                                    in_count, cursor, conn);
   if (n > 0) conn_sort_kernel<<<nblk(n, 256), 256, 0, st>>>(conn_off, in_count, n, conn);
+}
+
+// ------------------------------------------------------------ batch launchers --
+void launch_batch_grid(const double* xyz, int n, const int32_t* pos, const int32_t* cbase, int nj,
+                       const BatchGrid* bg, int64_t ncell, double* gen, unsigned long long* ext_keys,
+                       double* ext, int* bad, int32_t* cid, int32_t* count, int32_t* start,
+                       int32_t* dflag, int32_t* dprefix, long long* scan_tmp, cudaStream_t st) {
+  batch_ext_init_kernel<<<nblk(6 * (int64_t)nj, 256), 256, 0, st>>>(ext_keys, nj);
+  if (n > 0) batch_prep_kernel<<<nblk(n, 256), 256, 0, st>>>(xyz, n, pos, nj, bg, gen, ext_keys, bad);
+  batch_ext_finish_kernel<<<nblk(6 * (int64_t)nj, 256), 256, 0, st>>>(ext_keys, ext, nj);
+  if (n > 0) batch_cell_index_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, pos, nj, bg, cid, count);
+  scan_i32_to_i32(count, ncell, start, scan_tmp, st);
+  dense_flag_kernel<<<nblk(ncell, 256), 256, 0, st>>>(count, ncell, dflag);
+  scan_i32_to_i32(dflag, ncell, dprefix, scan_tmp, st);
+}
+
+size_t batch_sort_bytes(int n, int64_t ncell) { return grid_dense_sort_bytes(n, ncell); }
+
+cudaError_t launch_batch_sort(const double* gen, int n, const int32_t* pos, const int32_t* cbase, int nj,
+                              const BatchGrid* bg, int64_t ncell, const int32_t* cid, const int32_t* dflag,
+                              unsigned long long* key_a, unsigned long long* key_b, int32_t* val_a,
+                              int32_t* val_b, void* sort_tmp, size_t sort_bytes, double* sx, double* sy,
+                              double* sz, int32_t* sid, uint32_t* fkey, int32_t* start, cudaStream_t st) {
+  if (n > 0) {
+    int end_bit = FKEY_BITS;
+    while ((1ll << (end_bit - FKEY_BITS)) < ncell) end_bit++;
+    batch_key_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, pos, nj, bg, cid, dflag, key_a, val_a);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, key_a, key_b, val_a, val_b, n, 0,
+                                                    end_bit, st);
+    if (e != cudaSuccess) return e;
+    batch_gather_kernel<<<nblk(n, 256), 256, 0, st>>>(gen, n, key_b, val_b, pos, nj, sx, sy, sz, sid, fkey);
+  }
+  batch_local_starts_kernel<<<nblk(ncell, 256), 256, 0, st>>>(start, ncell, cbase, pos, nj);
+  return cudaGetLastError();
+}
+
+void launch_batch_csr(const FaceArrays& f, int64_t F, const int64_t* face_off, const int32_t* face_count,
+                      int n, const int32_t* pos, int nj, int32_t* in_count, int32_t* conn_count,
+                      cudaStream_t st) {
+  if (F > 0) batch_in_count_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, F, pos, nj, in_count);
+  if (n > 0) conn_count_kernel<<<nblk(n, 256), 256, 0, st>>>(face_count, in_count, n, conn_count);
+}
+
+void launch_batch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_off, const int64_t* conn_off,
+                           const int32_t* in_count, int32_t* cursor, int n, const int32_t* pos, int nj,
+                           int32_t* conn, cudaStream_t st) {
+  if (F > 0)
+    batch_conn_fill_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, face_off, conn_off, in_count,
+                                                         cursor, F, pos, nj, conn);
+  if (n > 0) conn_sort_kernel<<<nblk(n, 256), 256, 0, st>>>(conn_off, in_count, n, conn);
+}
+
+void launch_batch_localize(FaceArrays& f, int64_t F, const int64_t* face_off, int64_t* conn_off,
+                           const int32_t* conn_count, int32_t* conn, int n, const int32_t* pos, int nj,
+                           int64_t* fbase, int64_t* cbase_conn, cudaStream_t st) {
+  batch_bases_kernel<<<nblk(nj + 1, 256), 256, 0, st>>>(face_off, conn_off, pos, nj, fbase, cbase_conn);
+  if (F > 0) batch_local_faces_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, F, pos, nj);
+  if (conn_off != nullptr && n > 0)
+    batch_local_conn_kernel<<<nblk(n, 256), 256, 0, st>>>(conn_off, conn_count, conn, n, pos, nj, fbase,
+                                                          cbase_conn);
 }
 
 }  // namespace mv

@@ -124,6 +124,19 @@ struct Job {
   // ---- per-warp staging slots of the fused kernel for shells larger than its shared
   // buffer (slot = global warp index), or nullptr ----
   char* big;
+  // ---- batches: this tessellation's first position in the concatenated arrays of the
+  // batch (0 for a single build); staged faces and error cells carry it, so that the
+  // batch's finalize can find their tessellation ----
+  int32_t id_base;
+};
+
+// The tessellations of a batch build.  Tessellation j holds the sorted positions (and
+// input indices) [pos_base[j], pos_base[j + 1]) of the concatenated arrays; its Job
+// addresses its own slices, so every index inside it is local, as in the reference.
+struct JobTable {
+  const Job* jobs;          // [njobs], device
+  const int32_t* pos_base;  // [njobs + 1], device
+  int32_t njobs;
 };
 
 // One chunk of the staged path: cells at processing positions [item0, item0 + nitems)
@@ -144,6 +157,15 @@ struct StageJob {
   unsigned int* work;         // [3] work counters of the shell, clip and integral kernels
   int32_t* retry_list;        // positions the fused kernel builds afterwards
   unsigned int* retry_count;
+};
+
+// Grid of one tessellation of a batch (the batch grid kernels, mv_grid.cu).
+struct BatchGrid {
+  int G[3];
+  int dim;
+  double a[3], inv[3];
+  int32_t cbase;  // first batch-wide grid cell of the tessellation
+  int32_t pad;
 };
 
 // Normalised simulation volume, boundary planes (boundary.rs:14-47), uniform grid and

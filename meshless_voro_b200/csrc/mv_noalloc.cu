@@ -24,7 +24,7 @@
 #include "mv_internal.h"
 
 namespace mv {
-cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st);
+cudaError_t launch_cells(const Job& J, bool large, int blocks, cudaStream_t st, const JobTable& TB);
 int cells_blocks_per_sm_fast(int precision);
 int cells_blocks_per_sm_large(int precision);
 void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
@@ -247,7 +247,7 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
   J.status = C->status;
   J.stats = C->stats;
   const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
-  NA_CUDA(launch_cells(J, false, ds->sm_count * std::max(1, ds->bps_fast[pi]), st));
+  NA_CUDA(launch_cells(J, false, ds->sm_count * std::max(1, ds->bps_fast[pi]), st, JobTable{nullptr, nullptr, 0}));
   DevCounters hc;
   NA_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaStreamSynchronize(st));
@@ -260,7 +260,7 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
     L.ovf_list = at<int32_t>(B, O_OVFB);
     L.ovf_count = &C->ovf_count[1];
     const int blocks = std::min<int>(ds->sm_count * std::max(1, ds->bps_large[pi]), L.n_order);
-    NA_CUDA(launch_cells(L, true, blocks, st));
+    NA_CUDA(launch_cells(L, true, blocks, st, JobTable{nullptr, nullptr, 0}));
     NA_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
     NA_CUDA(cudaStreamSynchronize(st));
   }

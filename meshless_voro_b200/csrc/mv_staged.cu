@@ -76,21 +76,27 @@ __device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, in
   return (int)(__shfl_sync(FULL, tie[0], 0) / 27u) == self;
 }
 
-template <int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const __grid_constant__ Job J,
-                                                           const __grid_constant__ StageJob SJ) {
+template <int WARPS, bool MULTI>
+__global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB)
+    shell_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
+                 const __grid_constant__ JobTable TB) {
   __shared__ ShellBuf<SHELL_CMAX> bufs[WARPS];
   __shared__ double ext_s[6];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ShellBuf<SHELL_CMAX>& B = bufs[warp];
-  if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  if (threadIdx.x < 6) ext_s[threadIdx.x] = J0.ext[threadIdx.x];
   __syncthreads();
   for (;;) {
     int item = 0;
     if (lane == 0) item = (int)atomicAdd(SJ.work + 0, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= SJ.nitems) break;
-    const int spos = stage_pos(SJ, item);
+    const int gpos = stage_pos(SJ, item);
+    // the cell's tessellation (batch builds): its Job and its local position
+    const int jb = MULTI ? job_of(TB, gpos) : 0;
+    const Job& J = MULTI ? TB.jobs[jb] : J0;
+    const int spos = MULTI ? gpos - __ldg(TB.pos_base + jb) : gpos;
+    const double* ext = MULTI ? J.ext : ext_s;
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       if (lane == 0) SJ.info[item] = 0;
@@ -99,7 +105,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
     const D3 x = load_gen(J, self);
     bool all = false;
     double R = first_radius(J, x, lane);
-    int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
+    int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
     // the density estimate behind R is rough where the density varies: a shell that
     // overflows the list is pulled in, one far below a uniform region's ~92 candidates
     // (too small to close most cells) is widened, a few times at most
@@ -112,7 +118,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB) shell_kernel(const 
       else
         break;
       R *= f;
-      cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 32 * SHELL_CMAX);
+      cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
     }
     if (cnt > SHELL_CMAX || cnt == 0) {
       if (lane == 0) SJ.info[item] = -1;
@@ -144,21 +150,27 @@ constexpr int WIDE_MIN = 384;
 constexpr int WIDE_WARPS = 4;
 constexpr size_t WIDE_SMEM = sizeof(ShellBuf<WIDE_CMAX>) * WIDE_WARPS;
 
-template <int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, 3) shell_wide_kernel(const __grid_constant__ Job J,
-                                                                 const __grid_constant__ StageJob SJ) {
+template <int WARPS, bool MULTI>
+__global__ void __launch_bounds__(32 * WARPS, 3)
+    shell_wide_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
+                      const __grid_constant__ JobTable TB) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double ext_s[6];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ShellBuf<WIDE_CMAX>& B = reinterpret_cast<ShellBuf<WIDE_CMAX>*>(smem_raw)[warp];
-  if (threadIdx.x < 6) ext_s[threadIdx.x] = J.ext[threadIdx.x];
+  if (threadIdx.x < 6) ext_s[threadIdx.x] = J0.ext[threadIdx.x];
   __syncthreads();
   for (;;) {
     int item = 0;
     if (lane == 0) item = (int)atomicAdd(SJ.work + 0, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= SJ.nitems) break;
-    const int spos = stage_pos(SJ, item);
+    const int gpos = stage_pos(SJ, item);
+    // the cell's tessellation (batch builds): its Job and its local position
+    const int jb = MULTI ? job_of(TB, gpos) : 0;
+    const Job& J = MULTI ? TB.jobs[jb] : J0;
+    const int spos = MULTI ? gpos - __ldg(TB.pos_base + jb) : gpos;
+    const double* ext = MULTI ? J.ext : ext_s;
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       if (lane == 0) SJ.info[item] = 0;
@@ -167,7 +179,7 @@ __global__ void __launch_bounds__(32 * WARPS, 3) shell_wide_kernel(const __grid_
     const D3 x = load_gen(J, self);
     bool all = false;
     double R = 2.0 * first_radius(J, x, lane);
-    int cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 4 * WIDE_CMAX);
+    int cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 4 * WIDE_CMAX);
     for (int it = 0; it < 6; it++) {
       double f;
       if (cnt > WIDE_CMAX)
@@ -177,7 +189,7 @@ __global__ void __launch_bounds__(32 * WARPS, 3) shell_wide_kernel(const __grid_
       else
         break;
       R *= f;
-      cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext_s, &all, 4 * WIDE_CMAX);
+      cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 4 * WIDE_CMAX);
     }
     if (cnt > WIDE_CMAX || cnt == 0) {
       if (lane == 0) SJ.info[item] = -1;
@@ -524,9 +536,10 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   return CELL_DONE;
 }
 
-template <class T, int PREC, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_constant__ Job J,
-                                                                  const __grid_constant__ StageJob SJ) {
+template <class T, int PREC, int WARPS, bool MULTI>
+__global__ void __launch_bounds__(32 * WARPS, T::MINB)
+    clip_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
+                const __grid_constant__ JobTable TB) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ClipSmem<T>& S = reinterpret_cast<ClipSmem<T>*>(smem_raw)[warp];
@@ -538,7 +551,11 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
     if (lane == 0) item = (int)atomicAdd(SJ.work + 1, 1u);
     item = __shfl_sync(FULL, item, 0);
     if (item >= SJ.nitems) break;
-    const int spos = stage_pos(SJ, item);
+    const int gpos = stage_pos(SJ, item);
+    // the cell's tessellation (batch builds): its Job and its local position
+    const int jb = MULTI ? job_of(TB, gpos) : 0;
+    const Job& J = MULTI ? TB.jobs[jb] : J0;
+    const int spos = MULTI ? gpos - __ldg(TB.pos_base + jb) : gpos;
     const int self = __ldg(J.sid + spos);
     if (J.mask != nullptr && J.mask[self] == 0) {
       // VoronoiCell::default() (voronoi.rs:303-305)
@@ -570,10 +587,10 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
         SJ.rec_off[item] = -1;
         if (res == CELL_ERROR) {
           atomicCAS(J.status + STATUS_CODE, 0, err);
-          atomicMin(J.status + STATUS_CELL, self);
+          atomicMin(J.status + STATUS_CELL, self + J.id_base);
         } else {
           const unsigned k = atomicAdd(SJ.retry_count, 1u);
-          SJ.retry_list[k] = spos;
+          SJ.retry_list[k] = gpos;
         }
       }
     }
@@ -581,13 +598,14 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB) clip_kernel(const __grid_
   }
   __syncwarp();
   __syncthreads();
-  if (threadIdx.x < ST_COUNT && cnt[threadIdx.x]) atomicAdd(J.stats + threadIdx.x, cnt[threadIdx.x]);
+  if (threadIdx.x < ST_COUNT && cnt[threadIdx.x]) atomicAdd(J0.stats + threadIdx.x, cnt[threadIdx.x]);
 }
 
 // --------------------------------------------------------------- integrals --
-template <class T, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(const __grid_constant__ Job J,
-                                                               const __grid_constant__ StageJob SJ) {
+template <class T, int WARPS, bool MULTI>
+__global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB)
+    integrate_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
+                     const __grid_constant__ JobTable TB) {
   __shared__ TetScratch scratch[WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned done = 0;
@@ -598,7 +616,10 @@ __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(cons
     if (item >= SJ.nitems) break;
     const int64_t off = SJ.rec_off[item];
     if (off < 0) continue;
-    const int spos = stage_pos(SJ, item);
+    const int gpos = stage_pos(SJ, item);
+    const int jb = MULTI ? job_of(TB, gpos) : 0;
+    const Job& J = MULTI ? TB.jobs[jb] : J0;
+    const int spos = MULTI ? gpos - __ldg(TB.pos_base + jb) : gpos;
     const int self = __ldg(J.sid + spos);
     const D3 x = load_gen(J, self);
     const RecordView V(SJ.rec + off);
@@ -611,12 +632,12 @@ __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB) integrate_kernel(cons
         atomicExch(J.status + STATUS_FACE_OVERFLOW, 1);
       } else {
         atomicCAS(J.status + STATUS_CODE, 0, err);
-        atomicMin(J.status + STATUS_CELL, self);
+        atomicMin(J.status + STATUS_CELL, self + J.id_base);
       }
     }
     __syncwarp();
   }
-  if (lane == 0 && done) atomicAdd(J.stats + ST_CELLS, (unsigned long long)done);
+  if (lane == 0 && done) atomicAdd(J0.stats + ST_CELLS, (unsigned long long)done);
 }
 
 // ---------------------------------------------------------------- launchers --
@@ -633,15 +654,15 @@ static int occupancy(K k, int threads, size_t smem) {
 constexpr size_t CLIP_SMEM = sizeof(ClipSmem<TierClip>) * CLIP_WARPS;
 
 int stage_blocks_per_sm(int kernel, int precision) {
-  if (kernel == 0) return occupancy(shell_kernel<SHELL_WARPS>, 32 * SHELL_WARPS, 0);
-  if (kernel == 3) return occupancy(shell_wide_kernel<WIDE_WARPS>, 32 * WIDE_WARPS, WIDE_SMEM);
+  if (kernel == 0) return occupancy(shell_kernel<SHELL_WARPS, false>, 32 * SHELL_WARPS, 0);
+  if (kernel == 3) return occupancy(shell_wide_kernel<WIDE_WARPS, false>, 32 * WIDE_WARPS, WIDE_SMEM);
   if (kernel == 1)
     return precision == MV_PRECISION_FILTERED
-               ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>, 32 * CLIP_WARPS,
-                           CLIP_SMEM)
-               : occupancy(clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS>, 32 * CLIP_WARPS,
-                           CLIP_SMEM);
-  return occupancy(integrate_kernel<TierClip, INT_WARPS>, 32 * INT_WARPS, 0);
+               ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, false>,
+                           32 * CLIP_WARPS, CLIP_SMEM)
+               : occupancy(clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, false>,
+                           32 * CLIP_WARPS, CLIP_SMEM);
+  return occupancy(integrate_kernel<TierClip, INT_WARPS, false>, 32 * INT_WARPS, 0);
 }
 
 int stage_list_stride() { return SHELL_CMAX; }
@@ -649,31 +670,36 @@ int stage_wide_stride() { return WIDE_CMAX; }
 
 int64_t stage_record_words(int np, int nv) { return rec_words(np, nv); }
 
-cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, int blocks, cudaStream_t st) {
-  if (blocks < 1) blocks = 1;
+template <bool MULTI>
+static cudaError_t launch_stage_t(int kernel, const Job& J, const StageJob& SJ, const JobTable& TB,
+                                  int blocks, cudaStream_t st) {
   if (kernel == 0) {
-    shell_kernel<SHELL_WARPS><<<blocks, 32 * SHELL_WARPS, 0, st>>>(J, SJ);
+    shell_kernel<SHELL_WARPS, MULTI><<<blocks, 32 * SHELL_WARPS, 0, st>>>(J, SJ, TB);
   } else if (kernel == 3) {
-    auto k = shell_wide_kernel<WIDE_WARPS>;
+    auto k = shell_wide_kernel<WIDE_WARPS, MULTI>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WIDE_SMEM);
     if (e != cudaSuccess) return e;
-    k<<<blocks, 32 * WIDE_WARPS, WIDE_SMEM, st>>>(J, SJ);
+    k<<<blocks, 32 * WIDE_WARPS, WIDE_SMEM, st>>>(J, SJ, TB);
   } else if (kernel == 1) {
-    if (J.precision == MV_PRECISION_FILTERED) {
-      auto k = clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS>;
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
-      if (e != cudaSuccess) return e;
-      k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ);
-    } else {
-      auto k = clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS>;
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
-      if (e != cudaSuccess) return e;
-      k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ);
-    }
+    auto k = J.precision == MV_PRECISION_FILTERED
+                 ? clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, MULTI>
+                 : clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, MULTI>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ, TB);
   } else {
-    integrate_kernel<TierClip, INT_WARPS><<<blocks, 32 * INT_WARPS, 0, st>>>(J, SJ);
+    integrate_kernel<TierClip, INT_WARPS, MULTI><<<blocks, 32 * INT_WARPS, 0, st>>>(J, SJ, TB);
   }
   return cudaGetLastError();
+}
+
+// Launches stage kernel `kernel` (0 shell, 1 clip, 2 integrals, 3 wide shell); with a
+// job table (TB.jobs != nullptr) over the cells of a batch.
+cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, const JobTable& TB, int blocks,
+                         cudaStream_t st) {
+  if (blocks < 1) blocks = 1;
+  return TB.jobs != nullptr ? launch_stage_t<true>(kernel, J, SJ, TB, blocks, st)
+                            : launch_stage_t<false>(kernel, J, SJ, TB, blocks, st);
 }
 
 }  // namespace mv

@@ -161,6 +161,113 @@ class Context:
             raise N.MvError(rc, out.error_cell)
         return out
 
+    def build_batch(self, jobs, precision="filtered", face_mode=N.MV_FACES_OWNED, **kw) -> list:
+        """mv_context_build_batch: many tessellations in one build (host in, host out).
+        `jobs` holds dicts with generators, anchor, width, dimensionality, periodic and
+        optionally mask; returns one VoronoiArrays per job, each what build_arrays
+        returns for that job alone."""
+        g, m, descs = batch_inputs(jobs)
+        opts = make_options(precision, face_mode, **kw)
+        out = N.BatchVoronoi()
+        rc = N.lib().mv_context_build_batch(self._h, g.ctypes.data_as(C.c_void_p),
+                                            m.ctypes.data_as(C.c_void_p) if m is not None else None,
+                                            descs, len(jobs), C.byref(opts), C.byref(out))
+        if rc != N.MV_OK:
+            err = N.MvError(rc, out.error_cell)
+            err.error_job = out.error_job
+            raise err
+        return batch_arrays(out, descs, g, m)
+
+    def build_batch_device(self, d_generators: int, d_mask: int, descs, precision="filtered",
+                           face_mode=N.MV_FACES_OWNED, stream=None, **kw) -> N.BatchVoronoi:
+        """mv_context_build_batch_device: concatenated device inputs, device results."""
+        opts = make_options(precision, face_mode, stream=stream, **kw)
+        out = N.BatchVoronoi()
+        rc = N.lib().mv_context_build_batch_device(self._h, C.c_void_p(d_generators),
+                                                   C.c_void_p(d_mask) if d_mask else None, descs,
+                                                   len(descs), C.byref(opts), C.byref(out))
+        if rc != N.MV_OK:
+            err = N.MvError(rc, out.error_cell)
+            err.error_job = out.error_job
+            raise err
+        return out
+
+
+def batch_inputs(jobs):
+    """Concatenated generators, concatenated mask (or None) and the mv_job descriptors of a
+    sequence of tessellations, each a dict with generators, anchor, width, dimensionality,
+    periodic and optionally mask (the layout mv_context_build_batch reads)."""
+    gens, masks, descs = [], [], (N.Job * len(jobs))()
+    any_mask = any(j.get("mask") is not None for j in jobs)
+    for k, j in enumerate(jobs):
+        g = np.asarray(j["generators"], dtype=np.float64).reshape(-1, 3)
+        gens.append(g)
+        d = descs[k]
+        d.n = g.shape[0]
+        d.anchor[:] = list(_vec3(j["anchor"]))
+        d.width[:] = list(_vec3(j["width"]))
+        d.dimensionality = int(j["dimensionality"])
+        d.periodic = int(bool(j["periodic"]))
+        d.has_mask = int(j.get("mask") is not None)
+        if any_mask:
+            m = j.get("mask")
+            masks.append(np.ones(g.shape[0], np.uint8) if m is None
+                         else np.asarray(m, dtype=np.bool_).reshape(g.shape[0]).view(np.uint8))
+    g = np.ascontiguousarray(np.concatenate(gens) if gens else np.zeros((0, 3)))
+    m = np.ascontiguousarray(np.concatenate(masks)) if any_mask else None
+    return g, m, descs
+
+
+def batch_arrays(bv: N.BatchVoronoi, descs, generators: np.ndarray, mask_u8) -> list:
+    """Splits a host batch result into one VoronoiArrays per tessellation (copies)."""
+    nj = int(bv.n_jobs)
+    n, F, Cn = int(bv.n_cells), int(bv.n_faces), int(bv.n_connections)
+
+    def full(ptr, count, ctype, dtype, width=1):
+        if count == 0 or not ptr:
+            return np.zeros((0, width) if width > 1 else 0, dtype=dtype)
+        a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count * width,))
+        return a.reshape(count, width) if width > 1 else a
+
+    has_csr = bool(bv.cell_face_offset)
+    vol = full(bv.cell_volume, n, C.c_double, np.float64)
+    cen = full(bv.cell_centroid, n, C.c_double, np.float64, 3)
+    sr = full(bv.cell_safety_radius, n, C.c_double, np.float64)
+    foff = full(bv.cell_face_offset, n, C.c_int64, np.int64) if has_csr else None
+    fcnt = full(bv.cell_face_count, n, C.c_int32, np.int32) if has_csr else None
+    fl = full(bv.face_left, F, C.c_int32, np.int32)
+    fr = full(bv.face_right, F, C.c_int32, np.int32)
+    fa = full(bv.face_area, F, C.c_double, np.float64)
+    fc = full(bv.face_centroid, F, C.c_double, np.float64, 3)
+    fn = full(bv.face_normal, F, C.c_double, np.float64, 3)
+    fs = full(bv.face_shift_code, F, C.c_uint8, np.uint8)
+    conn = full(bv.cell_face_connections, Cn, C.c_int32, np.int32) if has_csr else None
+    co, fo, no = bv.job_cell_offset, bv.job_face_offset, bv.job_connection_offset
+    res = []
+    for j in range(nj):
+        c0, c1, f0, f1 = co[j], co[j + 1], fo[j], fo[j + 1]
+        d = descs[j]
+        dim = int(d.dimensionality)
+        loc = generators[c0:c1].copy()
+        if dim == 1:
+            loc[:, 1:] = 0.0
+        elif dim == 2:
+            loc[:, 2] = 0.0
+        if d.has_mask and mask_u8 is not None:
+            loc[mask_u8[c0:c1] == 0] = 0.0
+        res.append(VoronoiArrays(
+            n_cells=c1 - c0, anchor=np.array(d.anchor[:]), width=np.array(d.width[:]),
+            dimensionality=dim, periodic=bool(d.periodic),
+            cell_volume=vol[c0:c1].copy(), cell_centroid=cen[c0:c1].copy(), cell_loc=loc,
+            cell_safety_radius=sr[c0:c1].copy(),
+            cell_face_offset=foff[c0:c1].astype(np.int64) if has_csr else None,
+            cell_face_count=fcnt[c0:c1].astype(np.int64) if has_csr else None,
+            face_left=fl[f0:f1].astype(np.int64), face_right=fr[f0:f1].astype(np.int64),
+            face_area=fa[f0:f1].copy(), face_centroid=fc[f0:f1].copy(),
+            face_normal=fn[f0:f1].copy(), face_shift_code=fs[f0:f1].astype(np.int32),
+            cell_face_connections=conn[no[j]:no[j + 1]].astype(np.int64) if has_csr else None))
+    return res
+
 
 _default_ctx: Optional[Context] = None
 

@@ -84,3 +84,35 @@ def clustered(n=8388608, nclumps=2000, seed=4, periodic=True, dim=3):
         g[:, dim:] = 0.0
     return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=dim,
                 periodic=periodic, name=f"clustered_{n}_{nclumps}clumps_{'periodic' if periodic else 'rect'}")
+
+
+def batch_jobs(njobs=4096, seed=5, nmin=1000, nmax=200000):
+    """An uneven batch of independent tessellations (the batched configuration): per
+    job N log-uniform in [nmin, nmax]; 3D with probability 0.8, else 2D; i.i.d. uniform
+    points or a jittered lattice (U(+-0.25 spacing), about N points) with probability
+    1/2 each; box sides U[0.5, 2] at an anchor U[-1, 1]; periodic with probability 1/2;
+    and with probability 0.1 a partial build whose mask leaves out a random 25 % of the
+    generators.  Returns the list of job dicts (generators, anchor, width,
+    dimensionality, periodic, mask)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(njobs):
+        n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        dim = 3 if rng.uniform() < 0.8 else 2
+        width = rng.uniform(0.5, 2.0, 3)
+        anchor = rng.uniform(-1.0, 1.0, 3)
+        periodic = bool(rng.uniform() < 0.5)
+        if rng.uniform() < 0.5:
+            u = rng.uniform(0.0, 1.0, size=(n, 3))
+        else:
+            k = max(1, int(round(n ** (1.0 / dim))))
+            idx = np.indices((k,) * dim).reshape(dim, -1).T.astype(np.float64)
+            u = np.full((idx.shape[0], 3), 0.5)
+            u[:, :dim] = (idx + 0.5 + rng.uniform(-0.25, 0.25, size=idx.shape)) / k
+        g = anchor + u * width
+        if dim == 2:
+            g[:, 2] = anchor[2] + 0.5 * width[2]
+        mask = rng.uniform(size=len(g)) >= 0.25 if rng.uniform() < 0.1 else None
+        jobs.append(dict(generators=g, anchor=anchor, width=width, dimensionality=dim,
+                         periodic=periodic, mask=mask))
+    return jobs

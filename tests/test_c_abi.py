@@ -73,3 +73,44 @@ def test_no_device_is_reported_not_faked(lib):
         pass
     h = C.c_void_p()
     assert lib.mv_context_create(-1, C.byref(h)) == N.MV_ERR_NO_DEVICE
+
+
+def test_batch_descriptor_layout():
+    """mv_job / mv_batch_voronoi as the header lays them out, and the concatenated inputs
+    batch_inputs hands to mv_context_build_batch."""
+    assert C.sizeof(N.Job) == 8 + 48 + 16
+    assert N.Job.dimensionality.offset == 56 and N.Job.has_mask.offset == 64
+    assert C.sizeof(N.BatchVoronoi) == 4 * 8 + 3 * 8 + 12 * 8 + 2 * 8
+    import numpy as np
+    from meshless_voro_b200.voronoi import batch_inputs
+    rng = np.random.default_rng(0)
+    jobs = [dict(generators=rng.uniform(size=(5, 3)), anchor=[0, 0, 0], width=[1, 1, 1],
+                 dimensionality=3, periodic=True),
+            dict(generators=np.zeros((0, 3)), anchor=[1, 2, 3], width=[2, 2, 2],
+                 dimensionality=2, periodic=False),
+            dict(generators=rng.uniform(size=(4, 3)), anchor=[0, 0, 0], width=[1, 1, 1],
+                 dimensionality=1, periodic=False, mask=[True, False, True, True])]
+    g, m, d = batch_inputs(jobs)
+    assert g.shape == (9, 3) and g.flags.c_contiguous
+    assert np.array_equal(g[5:], jobs[2]["generators"])
+    assert m.dtype == np.uint8 and list(m) == [1] * 5 + [1, 0, 1, 1]
+    assert [x.n for x in d] == [5, 0, 4] and [x.has_mask for x in d] == [0, 0, 1]
+    assert list(d[1].anchor) == [1, 2, 3] and d[1].dimensionality == 2 and d[1].periodic == 0
+    g2, m2, _ = batch_inputs(jobs[:2])
+    assert m2 is None and g2.shape == (5, 3)
+
+
+def test_batch_workload_shape():
+    """The batched configuration: sizes, dimensionality and mask mix as specified."""
+    import numpy as np
+    from meshless_voro_b200 import workloads as W
+    jobs = W.batch_jobs(njobs=200, seed=9, nmin=50, nmax=2000)
+    n = np.array([len(j["generators"]) for j in jobs])
+    assert len(jobs) == 200 and n.min() >= 1 and n.max() <= 2000 * 1.2
+    assert 0.6 < np.mean([j["dimensionality"] == 3 for j in jobs]) < 0.95
+    for j in jobs:
+        g, a, w = j["generators"], j["anchor"], j["width"]
+        assert np.all(g >= a - 1e-12) and np.all(g <= a + w + 1e-12)
+        assert np.all((w >= 0.5) & (w <= 2.0))
+        if j["mask"] is not None:
+            assert j["mask"].shape == (len(g),)
