@@ -652,6 +652,8 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
 
     // ---- clear counters ----
     MV_CUDA(cudaMemsetAsync(C, 0, sizeof(DevCounters), st));
+    // the failing cell is a minimum over the failing cells: start above every index
+    MV_CUDA(cudaMemsetAsync(C->status + STATUS_CELL, 0x7f, sizeof(int32_t), st));
     MV_CUDA(cudaMemsetAsync(C->ext_keys, 0xff, 3 * sizeof(unsigned long long), st));
     MV_CUDA(cudaMemsetAsync(W.cell_count.p, 0, 4 * (ncell + 1), st));
     MV_CUDA(cudaMemsetAsync(W.cell_fill.p, 0, 4 * (ncell + 1), st));
@@ -915,13 +917,13 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
   mv_options_default(&o);
   if (opts_in) o = *opts_in;
   if (!ctx || !out || !jobs || njobs <= 0 || njobs > (1 << 24)) return MV_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->error_job = -1;
+  out->error_cell = -1;
   if (o.precision != MV_PRECISION_FP64 && o.precision != MV_PRECISION_FILTERED) return MV_ERR_ARG;
   if (o.face_mode != MV_FACES_OWNED && o.face_mode != MV_FACES_ALL) return MV_ERR_ARG;
   if (o.pipeline < MV_PIPELINE_AUTO || o.pipeline > MV_PIPELINE_FUSED || o.chunk_cells < 0)
     return MV_ERR_ARG;
-  std::memset(out, 0, sizeof(*out));
-  out->error_job = -1;
-  out->error_cell = -1;
   const int nj = (int)njobs;
   std::vector<Setup> S(nj);
   std::vector<int32_t> pos(nj + 1), cb(nj + 1);
@@ -1031,6 +1033,8 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
     face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_area.cap / 8));
     face_cap = std::min<int64_t>(face_cap, (int64_t)(W.st_cen.cap / 24));
     MV_CUDA(cudaMemsetAsync(C, 0, sizeof(DevCounters), st));
+    // the failing cell is a minimum over the failing cells: start above every index
+    MV_CUDA(cudaMemsetAsync(C->status + STATUS_CELL, 0x7f, sizeof(int32_t), st));
     MV_CUDA(cudaMemsetAsync(W.cell_count.p, 0, 4 * (ncell + 1), st));
 
     // ---- generators + batch grid ----
@@ -1449,6 +1453,9 @@ int build_batch_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mas
   if (any_mask && ntot > 0)
     MV_CUDA(cudaMemcpyAsync(ctx->ws.in_mask.p, mask, (size_t)ntot, cudaMemcpyHostToDevice, st));
   mv_batch_voronoi d;
+  std::memset(&d, 0, sizeof(d));
+  d.error_job = -1;
+  d.error_cell = -1;
   int rc = build_batch_device_impl(ctx, P<double>(ctx->ws.in_xyz), any_mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr,
                                    jobs, njobs, &o, &d);
   if (rc) {

@@ -178,6 +178,8 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
 
   // clear what must start at zero (the array keeps the previous call's contents)
   NA_CUDA(cudaMemsetAsync(C, 0, sizeof(DevCounters), st));
+  // the failing cell is a minimum over the failing cells: start above every index
+  NA_CUDA(cudaMemsetAsync(C->status + STATUS_CELL, 0x7f, sizeof(int32_t), st));
   NA_CUDA(cudaMemsetAsync(C->ext_keys, 0xff, 3 * sizeof(unsigned long long), st));
   NA_CUDA(cudaMemsetAsync(B + O_CCOUNT, 0, 4 * (ncell + 1), st));
   NA_CUDA(cudaMemsetAsync(B + O_CFILL, 0, 4 * (ncell + 1), st));

@@ -225,11 +225,14 @@ def test_reference_api_kats(gpu_ctx):
     assert len(ids) == cell.face_count() - sum(1 for f in cell.faces() if f.is_boundary())
 
 
-def test_duplicate_generators_raise(gpu_ctx):
-    g = [[0.2, 0.2, 0.2], [0.7, 0.7, 0.7], [0.2, 0.2, 0.2]]
+@pytest.mark.parametrize("pipeline", ["fused", "staged"])
+def test_duplicate_generators_raise(gpu_ctx, pipeline):
+    """convex_cell.rs:325-342 panics on a duplicate; the library names a duplicated cell."""
+    g = [[0.7, 0.7, 0.7], [0.2, 0.2, 0.2], [0.4, 0.5, 0.6], [0.2, 0.2, 0.2]]
     with pytest.raises(MvError) as e:
-        gpu_ctx.build_arrays(g, None, [0, 0, 0], [1, 1, 1], 3, False)
+        gpu_ctx.build_arrays(g, None, [0, 0, 0], [1, 1, 1], 3, False, **PIPELINES[pipeline])
     assert e.value.status == 2
+    assert e.value.error_cell in (1, 3)
 
 
 def test_empty_input(gpu_ctx):
