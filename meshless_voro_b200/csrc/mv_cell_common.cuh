@@ -291,6 +291,7 @@ struct ShellBuf {
   int32_t sstart[96];
   int32_t spref[97];
   int32_t gbin;                  // next bin of a staged shell (big shells), -1: none
+  int32_t total;                 // elements of the current shell (all its groups)
   uint8_t scode[96];
 };
 
@@ -562,8 +563,9 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
     if (bal) flush(__popc(bal), tot);
   };
   // the octree cells of dense cell (cx, cy, cz), image (mx, my, mz), that the shell
-  // [lo, R) reaches, at the level whose cells are at least R / 2 wide (at most five per
-  // axis); a cell that lies inside the inner radius holds no element of the shell
+  // [lo, R) reaches, at the level whose cells are at least half the shell's thickness
+  // wide (at most five per axis for a first shell, 33 for the thinnest); a cell that
+  // lies inside the inner radius holds no element of the shell
   auto dense_cell = [&](int cx, int cy, int cz, int mx, int my, int mz, int code) {
     const int64_t cc = (int64_t)cx + (int64_t)J.G[0] * (cy + (int64_t)J.G[1] * cz);
     const int32_t cs = __ldg(J.cell_start + cc), ce = __ldg(J.cell_start + cc + 1);
@@ -574,7 +576,10 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
     const int B = J.fbits, dim = J.dim;
     double hmin = J.gh[0];
     for (int i = 1; i < dim; i++) hmin = fmin(hmin, J.gh[i]);
-    const double r = 2.0 * hmin / R;
+    // the level: cells at least half as wide as the shell is thick (R / 8 at the
+    // thinnest), so that a thin shell's octree cells inside the inner radius drop out
+    const double span = fmax(R - sqrt(lo2), 0.125 * R);
+    const double r = 2.0 * hmin / span;
     const int L = r >= 2.0 ? min(B, ilogb(r)) : 0;
     const int nL = 1 << L;
     const int c3[3] = {cx, cy, cz}, m3[3] = {mx, my, mz};

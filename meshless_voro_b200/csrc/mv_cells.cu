@@ -242,7 +242,10 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     }
     if (cnt > T::CMAX && !staged) return CELL_OVERFLOW;
     // a staged shell is consumed in groups of bins (the cursor lives in shared memory)
-    if (lane == 0) S.u.g.sh.gbin = staged ? 0 : -1;
+    if (lane == 0) {
+      S.u.g.sh.gbin = staged ? 0 : -1;
+      S.u.g.sh.total = cnt;
+    }
     __syncwarp();
     if (staged) cnt = big_group<T::CMAX>(S.u.g.sh, big_slot(J), lane);
     for (;;) {
@@ -447,10 +450,19 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
     if (finished) break;
     if (all) break;
     if (sr < R * (1.0 - 1e-12)) break;
-    lo2 = R * R;
     // next shell: reach the safety radius, but at most double the radius, so that a
-    // cell that is still open does not gather (and then shrink) a domain-wide shell
-    R = fmin(fmax(R * 1.3, sr * 1.05), 2.0 * R);
+    // cell that is still open does not gather (and then shrink) a domain-wide shell;
+    // after a staged shell, no further than the density just seen fills about half a
+    // slot (a cell on a dense clump's surface streams the clump in many such shells)
+    double Rn = fmin(fmax(R * 1.3, sr * 1.05), 2.0 * R);
+    const int total = S.u.g.sh.total;
+    if (J.big != nullptr && total > T::CMAX) {
+      const double R3 = R * R * R, rin3 = lo2 * sqrt(lo2);
+      const double Rd = cbrt(R3 + (R3 - rin3) * (0.5 * (double)BIG_CAP / (double)total));
+      Rn = fmin(Rn, fmax(Rd, R * 1.0001));
+    }
+    lo2 = R * R;
+    R = Rn;
   }
   const int res = integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
   if (res == CELL_DONE && J.rec != nullptr &&
