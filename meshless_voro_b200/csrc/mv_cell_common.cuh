@@ -303,9 +303,9 @@ struct ShellBuf {
 // stream order and each group sorted by (d2, tie) continues the nearest-first stream
 // exactly.  Dense clumps make such shells common: the safety radius of a cell on the
 // surface of a compact clump takes in the whole clump.
-constexpr int BIG_CAP = 4096;
-constexpr int BIG_BINS = 256;
-constexpr size_t BIG_SLOT_BYTES = (size_t)BIG_CAP * 32 + BIG_BINS * 4;
+constexpr int BIG_CAP = 32768;
+constexpr int BIG_BINS = 2048;
+constexpr size_t BIG_SLOT_BYTES = (size_t)BIG_CAP * 32 + (size_t)BIG_BINS * 8;
 
 struct BigView {
   unsigned long long* keyA;  // the gathered shell (elements >= CMAX; the rest in shared)
@@ -315,6 +315,7 @@ struct BigView {
   int32_t* cposA;
   int32_t* cposB;
   int32_t* pinc;             // [BIG_BINS] inclusive prefix of the bin counts
+  int32_t* hist;             // [BIG_BINS] bin counts, then the bucketing cursors
 };
 
 __device__ __forceinline__ BigView big_view(char* slot) {
@@ -326,6 +327,7 @@ __device__ __forceinline__ BigView big_view(char* slot) {
   V.cposA = reinterpret_cast<int32_t*>(V.tieB + BIG_CAP);
   V.cposB = V.cposA + BIG_CAP;
   V.pinc = V.cposB + BIG_CAP;
+  V.hist = V.pinc + BIG_BINS;
   return V;
 }
 
@@ -336,48 +338,44 @@ __device__ __forceinline__ int big_bin(unsigned long long key, double lo2, doubl
 
 // Buckets the cnt (CMAX < cnt <= BIG_CAP) elements of a gathered shell [lo2, R2) into
 // the slot's B arrays by bin and returns the largest bin count; when that exceeds CMAX
-// nothing is bucketed and the caller narrows the shell instead.
+// nothing is bucketed and the caller narrows the shell instead.  The counters live in
+// the slot (global memory, private to the warp).
 template <int CMAX>
 __device__ __noinline__ int big_bucket(ShellBuf<CMAX>& B, char* slot, int lane, int cnt, double lo2,
                                        double R2) {
-  static_assert(CMAX * 8 >= BIG_BINS * 4, "bin counters live in the key array");
   const BigView V = big_view(slot);
   for (int i = lane; i < CMAX; i += 32) {
     V.keyA[i] = B.key[i];
     V.tieA[i] = B.tie[i];
     V.cposA[i] = B.cpos[i];
   }
-  __syncwarp();
-  int* H = reinterpret_cast<int*>(B.key);
-  for (int i = lane; i < BIG_BINS; i += 32) H[i] = 0;
+  for (int i = lane; i < BIG_BINS; i += 32) V.hist[i] = 0;
   __syncwarp();
   const double scale = (double)BIG_BINS / (R2 - lo2);
-  for (int i = lane; i < cnt; i += 32) atomicAdd(&H[big_bin(V.keyA[i], lo2, scale)], 1);
+  for (int i = lane; i < cnt; i += 32) atomicAdd(&V.hist[big_bin(V.keyA[i], lo2, scale)], 1);
   __syncwarp();
+  // lane l owns bins [PER l, PER (l + 1))
   constexpr int PER = BIG_BINS / 32;
-  int c[PER];
   int sum = 0, mx = 0;
-#pragma unroll
   for (int k = 0; k < PER; k++) {
-    c[k] = H[PER * lane + k];
-    sum += c[k];
-    mx = max(mx, c[k]);
+    const int c = V.hist[PER * lane + k];
+    sum += c;
+    mx = max(mx, c);
   }
   mx = (int)__reduce_max_sync(FULL, (unsigned)mx);
   if (mx > CMAX) return mx;
   int tot;
   int ex = warp_excl_scan(sum, lane, &tot);
-  __syncwarp();
-#pragma unroll
   for (int k = 0; k < PER; k++) {
-    H[PER * lane + k] = ex;
-    ex += c[k];
+    const int c = V.hist[PER * lane + k];
+    V.hist[PER * lane + k] = ex;
+    ex += c;
     V.pinc[PER * lane + k] = ex;
   }
   __syncwarp();
   for (int i = lane; i < cnt; i += 32) {
     const unsigned long long key = V.keyA[i];
-    const int pos = atomicAdd(&H[big_bin(key, lo2, scale)], 1);
+    const int pos = atomicAdd(&V.hist[big_bin(key, lo2, scale)], 1);
     V.keyB[pos] = key;
     V.tieB[pos] = V.tieA[i];
     V.cposB[pos] = V.cposA[i];
@@ -394,33 +392,36 @@ __device__ __noinline__ int big_group(ShellBuf<CMAX>& B, char* slot, int lane) {
   const BigView V = big_view(slot);
   const int b = B.gbin;
   const int base = b > 0 ? V.pinc[b - 1] : 0;
-  constexpr int PER = BIG_BINS / 32;
-  int nb = 0;
-#pragma unroll
-  for (int k = 0; k < PER; k++) {
-    const int kk = PER * lane + k;
-    nb += (kk >= b && V.pinc[kk] <= base + CMAX) ? 1 : 0;
+  // the last bin e >= b with pinc[e] <= base + CMAX (bin b alone holds <= CMAX)
+  int lo = b, hi = BIG_BINS - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (V.pinc[m] <= base + CMAX)
+      lo = m;
+    else
+      hi = m - 1;
   }
-  nb = (int)__reduce_add_sync(FULL, (unsigned)nb);
-  const int end = V.pinc[b + nb - 1];
+  const int end = V.pinc[lo];
   for (int i = lane; i < end - base; i += 32) {
     B.key[i] = V.keyB[base + i];
     B.tie[i] = V.tieB[base + i];
     B.cpos[i] = V.cposB[base + i];
   }
-  if (lane == 0) B.gbin = b + nb < BIG_BINS ? b + nb : -1;
+  if (lane == 0) B.gbin = lo + 1 < BIG_BINS ? lo + 1 : -1;
   __syncwarp();
   return end - base;
 }
 
-// The warp's staging slot (global warp index) and the count at which a gather stops.
+// The warp's staging slot (global warp index).
 __device__ __forceinline__ char* big_slot(const Job& J) {
   if (J.big == nullptr) return nullptr;
   const size_t w = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   return J.big + w * BIG_SLOT_BYTES;
 }
+// Elements a shell of the fused kernel may hold: a staging slot, or without slots the
+// count at which the gather stops (the shared buffer then takes CMAX of them).
 template <int CMAX>
-__device__ __forceinline__ int big_stop(const Job& J) {
+__device__ __forceinline__ int big_fits(const Job& J) {
   return J.big != nullptr ? BIG_CAP : 32 * CMAX;
 }
 

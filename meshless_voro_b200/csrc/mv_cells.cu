@@ -218,13 +218,14 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   for (int shell = 0; !finished; shell++) {
     if (shell > 0) WCNT(cc, ST_SHELLS, 1);
     bool all;
-    int cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, big_stop<T::CMAX>(J),
-                                          big_slot(J));
+    // what this shell may hold: the shared buffer, or a staging slot
+    const int fits = big_fits<T::CMAX>(J);
+    int cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, fits, big_slot(J));
     int shrink = 0;
     bool staged = false;
     for (;;) {
       if (cnt <= T::CMAX) break;
-      if (J.big != nullptr && cnt <= BIG_CAP &&
+      if (J.big != nullptr && cnt <= fits &&
           big_bucket<T::CMAX>(S.u.g.sh, big_slot(J), lane, cnt, lo2, R * R) <= T::CMAX) {
         staged = true;
         break;
@@ -233,11 +234,9 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
       // too many candidates: pull the outer radius in, so that the shell keeps about
       // half of what fits (by volume, at the density just seen)
       const double rin3 = lo2 * sqrt(lo2);
-      const double fits = J.big != nullptr ? (double)BIG_CAP : (double)T::CMAX;
-      const double g = fmin(fmax(0.5 * fits / (double)cnt, 1e-3), 0.7);
+      const double g = fmin(fmax(0.5 * (double)(J.big != nullptr ? fits : T::CMAX) / (double)cnt, 1e-3), 0.7);
       R = cbrt(rin3 + (R * R * R - rin3) * g);
-      cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, big_stop<T::CMAX>(J),
-                                        big_slot(J));
+      cnt = gather_shell<T::CMAX, true>(J, S.u.g.sh, lane, x, R, lo2, ext, &all, fits, big_slot(J));
       shrink++;
     }
     if (cnt > T::CMAX && !staged) return CELL_OVERFLOW;
