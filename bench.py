@@ -7,7 +7,8 @@ ordering and the cell -> face CSR.  Default workload: 256^3 = 16,777,216 i.i.d.
 uniform generators in the periodic unit box (seeded, synthetic).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision filtered|fp64]
-                  [--workload poisson_256|lattice_64|jitter_32|clustered|batch_4096]
+                  [--workload poisson_256|lattice_64|jitter_32|grid_64|grid_64_p95|clustered|
+                              batch_4096]
                   [--impl ours|reference]
                   [--pipeline auto|staged|fused]
 
@@ -74,6 +75,10 @@ def workload(name: str, seed: int):
         w = W.exact_lattice(64)
     elif name == "jitter_32":
         w = W.jittered_lattice_32(seed)
+    elif name == "grid_64":
+        w = W.grid_example(64, 0.0)
+    elif name == "grid_64_p95":
+        w = W.grid_example(64, 0.95, seed)
     elif name == "clustered":
         w = W.clustered(8388608, 2000, seed=seed)
     elif name.startswith("clustered_"):
@@ -87,6 +92,7 @@ def workload(name: str, seed: int):
 
 
 BATCH_GROUP_CELLS = 1 << 25  # generators per batch build (device memory bound)
+L2_FLUSH_BYTES = 256 << 20    # inputs below this are timed step by step with L2 flushed
 
 
 def batch_groups(jobs, cap=BATCH_GROUP_CELLS):
@@ -434,6 +440,10 @@ def main():
                                 w["dimensionality"], w["periodic"], precision=precision,
                                 stream=sp, pipeline=pipeline)
 
+    # inputs smaller than L2: flush it (write a 256 MB buffer) before every timed step
+    # and time each step alone
+    flush = torch.empty(1 << 26, dtype=torch.float32, device=dev) if 24 * n < L2_FLUSH_BYTES else None
+
     def timed(precision, steps, pipeline=args.pipeline):
         for _ in range(args.warmup):
             step(precision, pipeline)
@@ -442,14 +452,27 @@ def main():
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         per_step, stats, out = [], None, None
-        e0.record(stream)
-        for _ in range(steps):
-            out = step(precision, pipeline)
-            stats = ctx.last_stats()
-            per_step.append(stats)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, dev)
+        if flush is None:
+            e0.record(stream)
+            for _ in range(steps):
+                out = step(precision, pipeline)
+                stats = ctx.last_stats()
+                per_step.append(stats)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms_local = e0.elapsed_time(e1) / steps
+        else:
+            ms_local = 0.0
+            for _ in range(steps):
+                flush.fill_(1.0)
+                e0.record(stream)
+                out = step(precision, pipeline)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                stats = ctx.last_stats()
+                per_step.append(stats)
+                ms_local += e0.elapsed_time(e1) / steps
+        ms = max_over_ranks(ms_local, dist, dev)
         if world > 1:
             dist.barrier()
         # device times of the cell phase and its kernels (library CUDA events on `stream`)
@@ -551,7 +574,9 @@ def main():
                 "config": {"workload": w["name"], "n_generators": n, "periodic": w["periodic"],
                            "precision": args.precision, "pipeline": args.pipeline,
                            "parallelism": f"weak{world}",
-                           "cache": "inputs larger than L2 (403 MB generators)"},
+                           "cache": (f"inputs larger than L2 ({24 * n / 1e6:.0f} MB generators)"
+                                     if flush is None else
+                                     "L2 flushed (256 MB written) before each timed step")},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
                 "gpu_launches": int(stats["kernel_launches"]) * args.steps,
                 "clocks": clocks,

@@ -342,6 +342,10 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   SJ.rec_cap = rec_cap;
   SJ.retry_list = P<int32_t>(W.retry);
   SJ.retry_count = reinterpret_cast<unsigned int*>(ctr);
+  // cells that need the exact predicate skip the wide round: they join the list the
+  // fused kernel takes (the wide round's retry list; with kept records, the one list)
+  SJ.fused_list = keep_records ? SJ.retry_list : P<int32_t>(W.retry2);
+  SJ.fused_count = keep_records ? SJ.retry_count : reinterpret_cast<unsigned int*>(ctr + ctr2);
   for (int64_t c = 0; c < nchunks; c++) {
     SJ.item0 = (int32_t)(c * chunk);
     SJ.nitems = (int32_t)std::min<int64_t>(chunk, n - c * chunk);
@@ -359,11 +363,19 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
   }
   std::vector<unsigned long long> h(ctr_words);
-  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * ctr2, cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * (ctr2 + 1), cudaMemcpyDeviceToHost, st));
   MV_CUDA(cudaStreamSynchronize(st));
-  *n_retry = (int64_t)(h[0] & 0xffffffffull);
+  // the first round's retries: for the wide round, or with kept records (one list,
+  // exact cells included) for the fused kernel
+  const int64_t n_first = (int64_t)(h[0] & 0xffffffffull);
+  *n_retry = n_first;
   *n_wide = 0;
   *retry_order = P<int32_t>(W.retry);
+  if (!keep_records) {
+    // the fused kernel's list so far: the cells that needed the exact predicate
+    *retry_order = P<int32_t>(W.retry2);
+    *n_retry = (int64_t)(h[ctr2] & 0xffffffffull);
+  }
   for (int k = 0; k < 3; k++) ms_stage[k] = 0.0;
   for (int64_t c = 0; c < nchunks; c++) {
     for (int k = 0; k < 3; k++) {
@@ -372,14 +384,16 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
       ms_stage[k] += t;
     }
   }
-  if (!keep_records && *n_retry > 0) {
+  if (!keep_records && n_first > 0) {
     // the wide round over the retry list; what it cannot close goes to the fused kernel
-    const int64_t nr = *n_retry;
+    const int64_t nr = n_first;
     StageJob SW = SJ;
     SW.cstride = wstride;
     SW.order = P<int32_t>(W.retry);
     SW.retry_list = P<int32_t>(W.retry2);
     SW.retry_count = reinterpret_cast<unsigned int*>(ctr + ctr2);
+    SW.fused_list = SW.retry_list;
+    SW.fused_count = SW.retry_count;
     const int64_t nc = (nr + chunk2 - 1) / chunk2;
     for (int64_t c = 0; c < nc; c++) {
       SW.item0 = (int32_t)(c * chunk2);

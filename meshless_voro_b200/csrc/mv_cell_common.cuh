@@ -220,7 +220,8 @@ enum CellResult {
   CELL_ERROR = 2,
   CELL_FACE_OVERFLOW = 3,
   CELL_RETRY = 4,  // staged path: the cell needs the fused kernel (more neighbours)
-  CELL_REC_OVERFLOW = 5  // export build: no room for the cell's record
+  CELL_REC_OVERFLOW = 5,  // export build: no room for the cell's record
+  CELL_EXACT = 6  // staged path: a vertex needs the exact predicate; the fused kernel builds the cell
 };
 
 // Event counts of one cell, kept in warp-uniform registers (a lane-0 branch inside

@@ -155,8 +155,10 @@ struct StageJob {
   int64_t rec_cap;            // record words available to the chunk
   unsigned long long* rec_counter;
   unsigned int* work;         // [3] work counters of the shell, clip and integral kernels
-  int32_t* retry_list;        // positions the fused kernel builds afterwards
+  int32_t* retry_list;        // positions the next round (wide round, fused kernel) takes
   unsigned int* retry_count;
+  int32_t* fused_list;        // positions that go straight to the fused kernel (exact tests)
+  unsigned int* fused_count;
 };
 
 // Grid of one tessellation of a batch (the batch grid kernels, mv_grid.cu).

@@ -243,16 +243,15 @@ struct ClipSmem {
 };
 
 // Event counts of one clipped cell in two warp-uniform registers: a = neighbours
-// (16 bits) | planes (8) | serial rings (8), b = f32-undecided tests (16) | exact tests
-// (16).  A cell of the clip tier consumes at most 127 neighbours and holds at most 64
-// planes and 64 vertices, so no field overflows.
+// (16 bits) | planes (8) | serial rings (8), b = f32-undecided tests.  A cell of the
+// clip tier consumes at most 1023 neighbours and holds at most 64 planes and 64
+// vertices, so no field overflows (the clip kernel runs no exact test).
 struct ClipCount {
   unsigned a, b;
   __device__ void neighbours(unsigned v) { a += v; }
   __device__ void plane() { a += 1u << 16; }
   __device__ void serial_ring() { a += 1u << 24; }
   __device__ void undecided(unsigned v) { b += v; }
-  __device__ void exact(unsigned v) { b += v << 16; }
 };
 
 template <class T, int PREC>
@@ -392,7 +391,8 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
       const double d = dot(n, p);
       unsigned rm[T::NW];
-      int n_und = 0, n_ex = 0;
+      int n_und = 0;
+      bool need_exact = false;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
         const int q = lane + 32 * w;
@@ -411,20 +411,18 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           if (!decided) {
             n_und++;
             const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
-            if (fabs(c) < errb) {
-              removed = exact_clip(J, S, sl, x, ngb) < 0;
-              n_ex++;
-            } else {
-              removed = c < 0.0;
-            }
+            need_exact |= fabs(c) < errb;
+            removed = c < 0.0;
           }
         }
         rm[w] = __ballot_sync(FULL, removed);
       }
+      // inside the f64 band the reference decides with the exact in-sphere predicate
+      // (half_space.rs:40-47); its multi-limb arithmetic does not fit this kernel's
+      // register budget, so the fused kernel builds such cells (before any change here)
+      if (__any_sync(FULL, need_exact)) return CELL_EXACT;
       n_und = (int)__reduce_add_sync(FULL, (unsigned)n_und);
-      n_ex = (int)__reduce_add_sync(FULL, (unsigned)n_ex);
       if (PREC == MV_PRECISION_FILTERED) cc.undecided(n_und);
-      cc.exact(n_ex);
       int nrem = 0;
 #pragma unroll
       for (int w = 0; w < T::NW; w++) nrem += __popc(rm[w]);
@@ -577,17 +575,19 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB)
     __syncwarp();
     if (lane == 0) {
       if (res == CELL_DONE) {
-        const unsigned v[5] = {cc.a & 0xffffu, (cc.a >> 16) & 0xffu, cc.a >> 24, cc.b & 0xffffu,
-                               cc.b >> 16};
-        const int slot[5] = {ST_NEIGHBOURS, ST_PLANES, ST_SERIAL_RING, ST_F32_UNDECIDED, ST_EXACT};
+        const unsigned v[4] = {cc.a & 0xffffu, (cc.a >> 16) & 0xffu, cc.a >> 24, cc.b};
+        const int slot[4] = {ST_NEIGHBOURS, ST_PLANES, ST_SERIAL_RING, ST_F32_UNDECIDED};
 #pragma unroll
-        for (int i = 0; i < 5; i++)
+        for (int i = 0; i < 4; i++)
           if (v[i]) atomicAdd(&cnt[slot[i]], (unsigned long long)v[i]);
       } else {
         SJ.rec_off[item] = -1;
         if (res == CELL_ERROR) {
           atomicCAS(J.status + STATUS_CODE, 0, err);
           atomicMin(J.status + STATUS_CELL, self + J.id_base);
+        } else if (res == CELL_EXACT) {
+          const unsigned k = atomicAdd(SJ.fused_count, 1u);
+          SJ.fused_list[k] = gpos;
         } else {
           const unsigned k = atomicAdd(SJ.retry_count, 1u);
           SJ.retry_list[k] = gpos;

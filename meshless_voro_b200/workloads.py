@@ -116,3 +116,14 @@ def batch_jobs(njobs=4096, seed=5, nmin=1000, nmax=200000):
         jobs.append(dict(generators=g, anchor=anchor, width=width, dimensionality=dim,
                          periodic=periodic, mask=mask))
     return jobs
+
+
+def grid_example(count=64, pert=0.95, seed=1):
+    """The reference's examples/grid_3d.rs input: a count^3 perturbed grid (perturbation
+    pert, 0 for the perfect grid) in the non-periodic unit box -- the configuration its
+    published CPU times are quoted on."""
+    rng = np.random.default_rng(seed)
+    g = perturbed_grid([0, 0, 0], [1, 1, 1], count, pert, rng if pert else None)
+    kind = "perfect" if pert == 0 else f"perturbed{pert}"
+    return dict(generators=g, anchor=np.zeros(3), width=np.ones(3), dimensionality=3,
+                periodic=False, name=f"grid_{count}^3_{kind}_rect")
