@@ -453,10 +453,10 @@ __device__ __forceinline__ int job_of(const JobTable& T, int pos) {
 // segment that contains a dense cell (J.dprefix) is deferred: its cells are then
 // visited one by one, and a dense cell contributes the octree cells that the shell
 // reaches.  Without the ball test (all images enumerated) every cell counts whole.
-template <int CMAX, bool BIG = false>
-__device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
-                                         double lo2, const double* ext, bool* exhausted,
-                                         int stop, char* big = nullptr) {
+template <int CMAX, bool BIG, bool DENSE>
+__device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
+                                              double lo2, const double* ext, bool* exhausted,
+                                              int stop, char* big) {
   const double xa[3] = {x.x, x.y, x.z};
   int lo[3], hi[3];
   bool all = true;
@@ -663,8 +663,7 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
           int a = max(first, mx * Gx), b = min(last, mx * Gx + Gx - 1);
           if (a > b) continue;
           int c0 = a - mx * Gx, c1 = b - mx * Gx;
-          if (J.dprefix != nullptr &&
-              __ldg(J.dprefix + rowbase + c1 + 1) > __ldg(J.dprefix + rowbase + c0)) {
+          if (DENSE && __ldg(J.dprefix + rowbase + c1 + 1) > __ldg(J.dprefix + rowbase + c0)) {
             dfr[mx + 1] = c0 | (c1 << 16);
             continue;
           }
@@ -703,7 +702,7 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
     __syncwarp();
     flush(nsegs_total, total);
     // the deferred ranges, cell by cell (a sparse cell is one segment)
-    for (int im = 0; im < 3; im++) {
+    for (int im = 0; im < (DENSE ? 3 : 0); im++) {
       unsigned pend = __ballot_sync(FULL, dfr[im] >= 0);
       while (pend) {
         const int src = __ffs(pend) - 1;
@@ -728,6 +727,17 @@ __device__ __noinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int la
   }
   *exhausted = all && count <= stop && !__any_sync(FULL, beyond > 0);
   return count;
+}
+
+// gather_shell_impl without the dense-cell code when the build has no dense cell (the
+// uniform-density case keeps its registers), with it otherwise.
+template <int CMAX, bool BIG = false>
+__device__ __forceinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
+                                            double lo2, const double* ext, bool* exhausted, int stop,
+                                            char* big = nullptr) {
+  return J.dprefix != nullptr
+             ? gather_shell_impl<CMAX, BIG, true>(J, B, lane, x, R, lo2, ext, exhausted, stop, big)
+             : gather_shell_impl<CMAX, BIG, false>(J, B, lane, x, R, lo2, ext, exhausted, stop, big);
 }
 
 // Bitonic sort of the shell [0, n) by (key, tie) ascending, carrying cpos; n <= CMAX.
