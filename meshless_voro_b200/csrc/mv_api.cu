@@ -434,6 +434,16 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   return MV_OK;
 }
 
+// Staging-slot bytes of the fused kernel for a build of n cells: one slot per warp of
+// the largest fast-tier or large-tier grid the build can launch (a fast-tier grid has
+// at most one warp per cell, a large-tier one at most one block per cell).
+size_t big_slot_bytes(const mv_context* ctx, int pi, int64_t n) {
+  const int64_t sm = ctx->sm_count;
+  const int64_t fast = std::min<int64_t>(sm * std::max(1, ctx->bps_fast[pi]), (n + 3) / 4);
+  const int64_t large = std::min<int64_t>(sm * std::max(1, ctx->bps_large[pi]), n);
+  return cells_big_bytes((int)std::max<int64_t>(fast, 1), (int)std::max<int64_t>(large, 1));
+}
+
 // The cell phase of a build, after the grid: the staged rounds (or the fused kernel
 // alone), the fused kernel on what they left, the large tier on the cells that outgrew
 // the fast one; reads the device counters back into *hc.  J is the build's Job (for a
@@ -469,6 +479,7 @@ int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, c
   } else {
     if (n > 0) {
       int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+      blocks = (int)std::min<int64_t>(blocks, (n + 3) / 4);  // no idle warps (or slots)
       MV_CUDA(launch_cells(J, false, blocks, st, TB));
       (*launches)++;
     }
@@ -774,9 +785,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     J.stats = C->stats;
     const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
     {
-      const size_t bb = cells_big_bytes(ctx->sm_count * std::max(1, ctx->bps_fast[pi]),
-                                        ctx->sm_count * std::max(1, ctx->bps_large[pi]));
-      if (ensure(ctx, W.big, bb)) return MV_ERR_OOM;
+      if (ensure(ctx, W.big, big_slot_bytes(ctx, pi, n))) return MV_ERR_OOM;
       J.big = static_cast<char*>(W.big.p);
     }
     const bool staged = use_staged(o, n);
@@ -1020,11 +1029,7 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
   MV_CUDA(cudaMemcpyAsync(W.b_cbase.p, cb.data(), 4 * (size_t)(nj + 1), cudaMemcpyHostToDevice, st));
   MV_CUDA(cudaMemcpyAsync(W.b_grid.p, bg.data(), sizeof(BatchGrid) * (size_t)nj, cudaMemcpyHostToDevice, st));
   const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
-  {
-    const size_t bb = cells_big_bytes(ctx->sm_count * std::max(1, ctx->bps_fast[pi]),
-                                      ctx->sm_count * std::max(1, ctx->bps_large[pi]));
-    if (ensure(ctx, W.big, bb)) return MV_ERR_OOM;
-  }
+  if (ensure(ctx, W.big, big_slot_bytes(ctx, pi, ntot))) return MV_ERR_OOM;
   ratio = std::max(ratio, ctx->face_ratio_hint);
   int64_t face_cap = (int64_t)(ratio * (double)ntot) + 4096;
 
