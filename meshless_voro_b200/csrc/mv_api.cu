@@ -434,12 +434,20 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   return MV_OK;
 }
 
+// Fast-tier grid of the fused kernel for `cells` cells: the resident maximum, or fewer
+// blocks for small counts (at least four cells per warp, so that a small build's
+// warps, and their staging slots, stay few).
+int fused_blocks(const mv_context* ctx, int pi, int64_t cells) {
+  const int64_t full = (int64_t)ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(full, (cells + 15) / 16));
+}
+
 // Staging-slot bytes of the fused kernel for a build of n cells: one slot per warp of
-// the largest fast-tier or large-tier grid the build can launch (a fast-tier grid has
-// at most one warp per cell, a large-tier one at most one block per cell).
+// the largest fast-tier or large-tier grid the build can launch (fused_blocks; a
+// large-tier grid has at most one block per cell).
 size_t big_slot_bytes(const mv_context* ctx, int pi, int64_t n) {
   const int64_t sm = ctx->sm_count;
-  const int64_t fast = std::min<int64_t>(sm * std::max(1, ctx->bps_fast[pi]), (n + 3) / 4);
+  const int64_t fast = fused_blocks(ctx, pi, n);
   const int64_t large = std::min<int64_t>(sm * std::max(1, ctx->bps_large[pi]), n);
   return cells_big_bytes((int)std::max<int64_t>(fast, 1), (int)std::max<int64_t>(large, 1));
 }
@@ -468,8 +476,8 @@ int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, c
       Job Rj = J;
       Rj.order = retry_order;
       Rj.n_order = (int32_t)n_retry;
-      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
-      blocks = (int)std::min<int64_t>(blocks, (n_retry + 3) / 4);
+      // one warp per cell, within the grid the slots were sized for
+      const int blocks = (int)std::min<int64_t>(fused_blocks(ctx, pi, n), (n_retry + 3) / 4);
       MV_CUDA(cudaEventRecord(ctx->ev[7], st));
       MV_CUDA(launch_cells(Rj, false, blocks, st, TB));
       MV_CUDA(cudaEventRecord(ctx->ev[8], st));
@@ -478,9 +486,7 @@ int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, c
     }
   } else {
     if (n > 0) {
-      int blocks = ctx->sm_count * std::max(1, ctx->bps_fast[pi]);
-      blocks = (int)std::min<int64_t>(blocks, (n + 3) / 4);  // no idle warps (or slots)
-      MV_CUDA(launch_cells(J, false, blocks, st, TB));
+      MV_CUDA(launch_cells(J, false, fused_blocks(ctx, pi, n), st, TB));
       (*launches)++;
     }
     MV_CUDA(cudaEventRecord(ctx->ev[2], st));
