@@ -114,3 +114,53 @@ def test_batch_workload_shape():
         assert np.all((w >= 0.5) & (w <= 2.0))
         if j["mask"] is not None:
             assert j["mask"].shape == (len(g),)
+
+
+def test_batch_result_split():
+    """batch_arrays splits a concatenated batch result by its per-tessellation offsets
+    (no GPU: the result is assembled in host memory)."""
+    import numpy as np
+    from meshless_voro_b200.voronoi import batch_arrays, batch_inputs
+    rng = np.random.default_rng(1)
+    jobs = [dict(generators=rng.uniform(size=(3, 3)), anchor=[0, 0, 0], width=[1, 1, 1],
+                 dimensionality=3, periodic=True),
+            dict(generators=rng.uniform(size=(2, 3)), anchor=[0, 0, 0], width=[2, 2, 2],
+                 dimensionality=2, periodic=False, mask=[True, False])]
+    g, m, descs = batch_inputs(jobs)
+    n, F, Cn = 5, 7, 9
+    keep = []
+
+    def buf(a):
+        a = np.ascontiguousarray(a)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    bv = N.BatchVoronoi()
+    bv.n_jobs, bv.n_cells, bv.n_faces, bv.n_connections = 2, n, F, Cn
+    offs = [(C.c_int64 * 3)(0, 3, 5), (C.c_int64 * 3)(0, 4, 7), (C.c_int64 * 3)(0, 6, 9)]
+    bv.job_cell_offset, bv.job_face_offset, bv.job_connection_offset = [
+        C.cast(o, C.POINTER(C.c_int64)) for o in offs]
+    bv.cell_volume = buf(np.arange(n, dtype=np.float64))
+    bv.cell_centroid = buf(np.arange(3 * n, dtype=np.float64))
+    bv.cell_safety_radius = buf(np.ones(n))
+    bv.cell_face_offset = buf(np.array([0, 2, 4, 0, 2], dtype=np.int64))
+    bv.cell_face_count = buf(np.array([2, 2, 2, 2, 1], dtype=np.int32))
+    bv.face_left = buf(np.array([0, 0, 1, 2, 0, 0, 1], dtype=np.int32))
+    bv.face_right = buf(np.array([1, 2, 2, -1, 1, -1, -1], dtype=np.int32))
+    bv.face_area = buf(np.arange(F, dtype=np.float64))
+    bv.face_centroid = buf(np.zeros(3 * F))
+    bv.face_normal = buf(np.zeros(3 * F))
+    bv.face_shift_code = buf(np.full(F, 13, dtype=np.uint8))
+    bv.cell_face_connections = buf(np.array([0, 1, 0, 2, 1, 3, 0, 1, 2], dtype=np.int32))
+    a, b = batch_arrays(bv, descs, g, m)
+    assert a.n_cells == 3 and b.n_cells == 2
+    assert list(a.cell_volume) == [0, 1, 2] and list(b.cell_volume) == [3, 4]
+    assert list(a.face_area) == [0, 1, 2, 3] and list(b.face_area) == [4, 5, 6]
+    assert list(b.face_left) == [0, 0, 1] and list(b.face_right) == [1, -1, -1]
+    assert list(a.cell_face_connections) == [0, 1, 0, 2, 1, 3]
+    assert list(b.cell_face_connections) == [0, 1, 2]
+    assert list(b.cell_face_offset) == [0, 2]
+    assert b.dimensionality == 2 and not b.periodic and list(b.width) == [2, 2, 2]
+    # 2D: z of the generator zeroed; the masked-out cell's location is zero
+    assert b.cell_loc[0, 2] == 0.0 and np.all(b.cell_loc[1] == 0.0)
+    assert np.array_equal(a.cell_loc, jobs[0]["generators"])
