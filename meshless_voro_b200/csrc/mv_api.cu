@@ -442,6 +442,38 @@ int fused_blocks(const mv_context* ctx, int pi, int64_t cells) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(full, (cells + 15) / 16));
 }
 
+// The tessellation-specific geometry of a Job: its grid, boundary planes (boundary.rs:
+// 14-47), iloc frame (boundary.rs:49-64), periodic image offsets (rtree_nn.rs:27-33,
+// 86), first shell radius and Morton key width.
+void set_job_geometry(Job& J, const Setup& s) {
+  for (int i = 0; i < 3; i++) {
+    J.G[i] = s.G[i];
+    J.ga[i] = s.anchor[i];
+    J.gw[i] = s.width[i];
+    J.gh[i] = s.gh[i];
+    J.ginv[i] = s.ginv[i];
+    J.geps[i] = s.geps[i];
+    J.iloc_a[i] = s.iloc_a[i];
+    J.iloc_inv[i] = s.iloc_inv[i];
+  }
+  J.dim = s.dim;
+  J.periodic = s.periodic;
+  J.R0 = s.R0;
+  J.fbits = fkey_bits(s.dim);
+  for (int c = 0; c < 27; c++) {
+    const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
+    for (int i = 0; i < 3; i++) {
+      const double q = (double)(-m[i]) * s.width[i];
+      J.qshift[c][i] = q;
+      J.shift[c][i] = -q;
+    }
+  }
+  for (int k = 0; k < 6; k++) {
+    for (int i = 0; i < 3; i++) J.bn[k][i] = s.bn[k][i], J.bp[k][i] = s.bp[k][i];
+    J.bd[k] = s.bd[k];
+  }
+}
+
 // Staging-slot bytes of the fused kernel for a build of n cells: one slot per warp of
 // the largest fast-tier or large-tier grid the build can launch (fused_blocks; a
 // large-tier grid has at most one block per cell).
@@ -739,36 +771,11 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     }
     J.mask = d_mask;
     J.n = ni;
-    J.dim = s.dim;
-    J.periodic = s.periodic;
     J.face_mode = o.face_mode;
     J.precision = o.precision;
-    for (int i = 0; i < 3; i++) {
-      J.G[i] = s.G[i];
-      J.ga[i] = s.anchor[i];
-      J.gw[i] = s.width[i];
-      J.gh[i] = s.gh[i];
-      J.ginv[i] = s.ginv[i];
-      J.geps[i] = s.geps[i];
-      J.iloc_a[i] = s.iloc_a[i];
-      J.iloc_inv[i] = s.iloc_inv[i];
-    }
+    set_job_geometry(J, s);
     J.ext = C->ext;
-    J.R0 = s.R0;
-    J.fbits = fkey_bits(s.dim);
     J.ppc_mean = (double)std::max<int64_t>(n, 1) / (double)ncell;
-    for (int c = 0; c < 27; c++) {
-      const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
-      for (int i = 0; i < 3; i++) {
-        const double q = (double)(-m[i]) * s.width[i];
-        J.qshift[c][i] = q;
-        J.shift[c][i] = -q;
-      }
-    }
-    for (int k = 0; k < 6; k++) {
-      for (int i = 0; i < 3; i++) J.bn[k][i] = s.bn[k][i], J.bp[k][i] = s.bp[k][i];
-      J.bd[k] = s.bd[k];
-    }
     J.volume = P<double>(W.volume);
     J.centroid = P<double>(W.centroid);
     J.safety_radius = P<double>(W.sr);
@@ -1092,38 +1099,13 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
       J.dprefix = P<int32_t>(W.dprefix) + cbj;
       J.cell_dense = P<int32_t>(W.dflag) + cbj;
       J.fkey = P<uint32_t>(W.fkey) + pb;
-      J.fbits = fkey_bits(sj.dim);
       J.mask = jobs[j].has_mask ? d_mask + pb : nullptr;
       J.n = (int32_t)jobs[j].n;
-      J.dim = sj.dim;
-      J.periodic = sj.periodic;
       J.face_mode = o.face_mode;
       J.precision = o.precision;
-      for (int i = 0; i < 3; i++) {
-        J.G[i] = sj.G[i];
-        J.ga[i] = sj.anchor[i];
-        J.gw[i] = sj.width[i];
-        J.gh[i] = sj.gh[i];
-        J.ginv[i] = sj.ginv[i];
-        J.geps[i] = sj.geps[i];
-        J.iloc_a[i] = sj.iloc_a[i];
-        J.iloc_inv[i] = sj.iloc_inv[i];
-      }
+      set_job_geometry(J, sj);
       J.ext = P<double>(W.b_ext) + 6 * j;
-      J.R0 = sj.R0;
       J.ppc_mean = (double)std::max<int64_t>(jobs[j].n, 1) / (double)(cb[j + 1] - cb[j] - 1);
-      for (int c = 0; c < 27; c++) {
-        const int m[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
-        for (int i = 0; i < 3; i++) {
-          const double q = (double)(-m[i]) * sj.width[i];
-          J.qshift[c][i] = q;
-          J.shift[c][i] = -q;
-        }
-      }
-      for (int k = 0; k < 6; k++) {
-        for (int i = 0; i < 3; i++) J.bn[k][i] = sj.bn[k][i], J.bp[k][i] = sj.bp[k][i];
-        J.bd[k] = sj.bd[k];
-      }
       J.volume = P<double>(W.volume) + pb;
       J.centroid = P<double>(W.centroid) + 3 * pb;
       J.safety_radius = P<double>(W.sr) + pb;
