@@ -467,6 +467,54 @@ class Voronoi:
     def dimensionality(self) -> int:
         return self.arrays.dimensionality
 
+    def hdf5_datasets(self) -> dict:
+        """The datasets Voronoi::write_to_hdf5 writes (voronoi.rs:432-491), by HDF5 path:
+        Cells/{Volume, FaceConnectionsOffset, FaceCount, Centroid, Generator},
+        Faces/{Area, Centroid, Normal} (and Start, End for 2D) and CellFaceConnections,
+        in its types (usize as uint64).  The 2D face end points are
+        centroid -/+ 0.5 * area * (normal x Z) in glam's operation order
+        (voronoi.rs:462-483), so they are the reference's binary64 values."""
+        a = self.arrays
+        if a.cell_face_connections is None:
+            raise ValueError("the HDF5 layout needs the cell -> face connections (MV_FACES_OWNED)")
+        d = {
+            "Cells/Volume": np.asarray(a.cell_volume, dtype=np.float64),
+            "Cells/FaceConnectionsOffset": np.asarray(a.cell_face_offset, dtype=np.uint64),
+            "Cells/FaceCount": np.asarray(a.cell_face_count, dtype=np.uint64),
+            "Cells/Centroid": np.asarray(a.cell_centroid, dtype=np.float64).reshape(-1, 3),
+            "Cells/Generator": np.asarray(a.cell_loc, dtype=np.float64).reshape(-1, 3),
+            "Faces/Area": np.asarray(a.face_area, dtype=np.float64),
+            "Faces/Centroid": np.asarray(a.face_centroid, dtype=np.float64).reshape(-1, 3),
+            "Faces/Normal": np.asarray(a.face_normal, dtype=np.float64).reshape(-1, 3),
+        }
+        if a.dimensionality == 2:
+            n, c = d["Faces/Normal"], d["Faces/Centroid"]
+            # DVec3::cross(n, Z): (n.y z - Z.y n.z, n.z Z.x - Z.z n.x, n.x Z.y - Z.x n.y)
+            cross = np.stack([n[:, 1] * 1.0 - 0.0 * n[:, 2], n[:, 2] * 0.0 - 1.0 * n[:, 0],
+                              n[:, 0] * 0.0 - 0.0 * n[:, 1]], axis=1)
+            direction = d["Faces/Area"][:, None] * cross
+            d["Faces/Start"] = c - 0.5 * direction
+            d["Faces/End"] = c + 0.5 * direction
+        d["CellFaceConnections"] = np.asarray(a.cell_face_connections, dtype=np.uint64)
+        return d
+
+    def write_to_hdf5(self, filename) -> None:
+        """Voronoi::write_to_hdf5 (voronoi.rs:432-491): groups Cells and Faces and the
+        top-level CellFaceConnections, through h5py (the crate needs its `hdf5` feature
+        for this; here the h5py package)."""
+        try:
+            import h5py
+        except ImportError as e:
+            raise RuntimeError("write_to_hdf5 needs the h5py package, which is not installed; "
+                               "save_datasets writes the same datasets to an .npz") from e
+        with h5py.File(filename, "w") as f:
+            for path, data in self.hdf5_datasets().items():
+                f.create_dataset(path, data=data)
+
+    def save_datasets(self, filename) -> None:
+        """The datasets of write_to_hdf5 in an .npz archive, keyed by their HDF5 paths."""
+        np.savez(filename, **self.hdf5_datasets())
+
     def periodic(self) -> bool:
         return self.arrays.periodic
 
