@@ -38,7 +38,7 @@ namespace mv {
 #define MV_FAST_MINB 5
 #endif
 #ifndef MV_FAST_KMAX
-#define MV_FAST_KMAX 8
+#define MV_FAST_KMAX 16
 #endif
 using TierFast = Tier<64, 64, 128, MV_FAST_KMAX, uint8_t, MV_FAST_MINB>;
 using TierLarge = Tier<512, 512, 512, 32, uint16_t, 1>;
