@@ -35,7 +35,7 @@ namespace mv {
 
 // Resident blocks per SM the fast tier is compiled for (sets its register budget).
 #ifndef MV_FAST_MINB
-#define MV_FAST_MINB 5
+#define MV_FAST_MINB 4
 #endif
 #ifndef MV_FAST_KMAX
 #define MV_FAST_KMAX 16
