@@ -66,3 +66,19 @@ def test_single_process_identity():
     import bench
     assert bench.max_over_ranks(7.5, None, None) == 7.5
     assert bench.aggregate_cells_per_s(1, 1000, 1.0) == pytest.approx(1e6)
+
+
+def test_batch_groups_split_by_generators():
+    """bench.py's batched workload: consecutive groups of at most `cap` generators, a job
+    larger than cap alone, order and membership kept."""
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    sizes = [5, 3, 9, 2, 2, 20, 1, 4]
+    jobs = [dict(generators=np.zeros((k, 3)), tag=i) for i, k in enumerate(sizes)]
+    groups = bench.batch_groups(jobs, cap=10)
+    assert [j["tag"] for g in groups for j in g] == list(range(len(sizes)))
+    for g in groups:
+        total = sum(len(j["generators"]) for j in g)
+        assert total <= 10 or len(g) == 1
+    assert [[j["tag"] for j in g] for g in groups] == [[0, 1], [2], [3, 4], [5], [6, 7]]
