@@ -167,8 +167,9 @@ def run_batch(args, rank, world):
     def step():
         stats, F, Cn = [], 0, 0
         for gr in groups:
-            out = ctx.build_batch_device(gr["gd"].data_ptr(), gr["md"].data_ptr() if gr["md"] is not None else 0,
-                                         gr["descs"], precision=args.precision, stream=sp)
+            d_mask = gr["md"].data_ptr() if gr["md"] is not None else 0
+            out = ctx.build_batch_device(gr["gd"].data_ptr(), d_mask, gr["descs"],
+                                         precision=args.precision, stream=sp)
             F += int(out.n_faces)
             Cn += int(out.n_connections)
             stats.append(ctx.last_stats())

@@ -1082,7 +1082,9 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
                               W.dsort_tmp.p, W.dsort_tmp.cap, P<double>(W.sx), P<double>(W.sy),
                               P<double>(W.sz), P<int32_t>(W.sid), P<uint32_t>(W.fkey),
                               P<int32_t>(W.cell_start), st));
-    launches += 19;  // ext init/prep/finish, cell index, 2 x 3 scan kernels, dense flags, keys, sort, gather, starts
+    // ext init / prep / finish, cell index, 2 x 3 scan kernels, dense flags, keys, sort,
+    // gather, starts
+    launches += 19;
 
     // ---- one Job per tessellation, addressing its slices ----
     for (int j = 0; j < nj; j++) {
@@ -1214,7 +1216,8 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
   ctx->bj_cell.assign(pos.begin(), pos.end());
   ctx->bj_face.assign(nj + 1, 0);
   ctx->bj_conn.assign(nj + 1, 0);
-  MV_CUDA(cudaMemcpyAsync(ctx->bj_face.data(), W.b_fbase.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaMemcpyAsync(ctx->bj_face.data(), W.b_fbase.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost,
+                          st));
   if (owned)
     MV_CUDA(cudaMemcpyAsync(ctx->bj_conn.data(), W.b_cbconn.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost,
                             st));
@@ -1463,8 +1466,8 @@ int build_batch_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mas
   std::memset(&d, 0, sizeof(d));
   d.error_job = -1;
   d.error_cell = -1;
-  int rc = build_batch_device_impl(ctx, P<double>(ctx->ws.in_xyz), any_mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr,
-                                   jobs, njobs, &o, &d);
+  int rc = build_batch_device_impl(ctx, P<double>(ctx->ws.in_xyz),
+                                   any_mask ? P<uint8_t>(ctx->ws.in_mask) : nullptr, jobs, njobs, &o, &d);
   if (rc) {
     *out = d;
     return rc;

@@ -374,8 +374,9 @@ __global__ void batch_ext_finish_kernel(const unsigned long long* ext_keys, doub
 }
 
 // grid cell (batch-wide index) of each generator, and the cell counts
-__global__ void batch_cell_index_kernel(const double* __restrict__ gen, int n, const int32_t* __restrict__ pos,
-                                        int nj, const BatchGrid* __restrict__ bg, int32_t* __restrict__ cid,
+__global__ void batch_cell_index_kernel(const double* __restrict__ gen, int n,
+                                        const int32_t* __restrict__ pos, int nj,
+                                        const BatchGrid* __restrict__ bg, int32_t* __restrict__ cid,
                                         int32_t* __restrict__ count) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -444,7 +445,8 @@ __global__ void batch_local_starts_kernel(int32_t* __restrict__ start, int64_t n
 // until the CSR is built; right indices are local to the tessellation
 __global__ void batch_in_count_kernel(const int32_t* __restrict__ left, const int32_t* __restrict__ right,
                                       const uint8_t* __restrict__ code, int64_t F,
-                                      const int32_t* __restrict__ pos, int nj, int32_t* __restrict__ in_count) {
+                                      const int32_t* __restrict__ pos, int nj,
+                                      int32_t* __restrict__ in_count) {
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   const int r = right[f];
@@ -480,14 +482,15 @@ __global__ void batch_bases_kernel(const int64_t* __restrict__ face_off, const i
 }
 
 // faces: left becomes local; CSR: offsets and face indices become local
-__global__ void batch_local_faces_kernel(int32_t* __restrict__ left, int64_t F, const int32_t* __restrict__ pos,
-                                         int nj) {
+__global__ void batch_local_faces_kernel(int32_t* __restrict__ left, int64_t F,
+                                         const int32_t* __restrict__ pos, int nj) {
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   left[f] -= pos[batch_find(pos, nj, left[f])];
 }
 
-__global__ void batch_local_conn_kernel(int64_t* __restrict__ conn_off, const int32_t* __restrict__ conn_count,
+__global__ void batch_local_conn_kernel(int64_t* __restrict__ conn_off,
+                                        const int32_t* __restrict__ conn_count,
                                         int32_t* __restrict__ conn, int n, const int32_t* __restrict__ pos,
                                         int nj, const int64_t* __restrict__ fbase,
                                         const int64_t* __restrict__ cbase_conn) {
@@ -656,7 +659,8 @@ cudaError_t launch_batch_sort(const double* gen, int n, const int32_t* pos, cons
 void launch_batch_csr(const FaceArrays& f, int64_t F, const int64_t* face_off, const int32_t* face_count,
                       int n, const int32_t* pos, int nj, int32_t* in_count, int32_t* conn_count,
                       cudaStream_t st) {
-  if (F > 0) batch_in_count_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, F, pos, nj, in_count);
+  if (F > 0)
+    batch_in_count_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, F, pos, nj, in_count);
   if (n > 0) conn_count_kernel<<<nblk(n, 256), 256, 0, st>>>(face_count, in_count, n, conn_count);
 }
 
@@ -664,8 +668,8 @@ void launch_batch_csr_fill(const FaceArrays& f, int64_t F, const int64_t* face_o
                            const int32_t* in_count, int32_t* cursor, int n, const int32_t* pos, int nj,
                            int32_t* conn, cudaStream_t st) {
   if (F > 0)
-    batch_conn_fill_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, face_off, conn_off, in_count,
-                                                         cursor, F, pos, nj, conn);
+    batch_conn_fill_kernel<<<nblk(F, 256), 256, 0, st>>>(f.left, f.right, f.code, face_off, conn_off,
+                                                         in_count, cursor, F, pos, nj, conn);
   if (n > 0) conn_sort_kernel<<<nblk(n, 256), 256, 0, st>>>(conn_off, in_count, n, conn);
 }
 

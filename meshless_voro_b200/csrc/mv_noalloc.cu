@@ -249,7 +249,8 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
   J.status = C->status;
   J.stats = C->stats;
   const int pi = o.precision == MV_PRECISION_FILTERED ? 1 : 0;
-  NA_CUDA(launch_cells(J, false, ds->sm_count * std::max(1, ds->bps_fast[pi]), st, JobTable{nullptr, nullptr, 0}));
+  NA_CUDA(launch_cells(J, false, ds->sm_count * std::max(1, ds->bps_fast[pi]), st,
+                       JobTable{nullptr, nullptr, 0}));
   DevCounters hc;
   NA_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaStreamSynchronize(st));
