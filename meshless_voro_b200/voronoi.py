@@ -193,6 +193,46 @@ class Context:
         return out
 
 
+class _DeviceArray:
+    """A device pointer seen through __cuda_array_interface__ (no copy, not owned)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+_DEVICE_FIELDS = (
+    # name, element type, per-row width, row count ("n", "F" or "C")
+    ("cell_volume", "<f8", 1, "n"), ("cell_centroid", "<f8", 3, "n"),
+    ("cell_safety_radius", "<f8", 1, "n"), ("cell_face_offset", "<i8", 1, "n"),
+    ("cell_face_count", "<i4", 1, "n"), ("face_left", "<i4", 1, "F"),
+    ("face_right", "<i4", 1, "F"), ("face_area", "<f8", 1, "F"),
+    ("face_centroid", "<f8", 3, "F"), ("face_normal", "<f8", 3, "F"),
+    ("face_shift_code", "|u1", 1, "F"), ("cell_face_connections", "<i4", 1, "C"),
+)
+
+
+def device_tensors(dv, device=None) -> dict:
+    """Zero-copy torch views of a device result (mv_device_voronoi, or a batch result's
+    device arrays): one tensor per array, valid until the context's next build.  Arrays
+    the build did not produce (the CSR of an MV_FACES_ALL build) are absent."""
+    import torch
+    rows = {"n": int(dv.n_cells), "F": int(dv.n_faces), "C": int(dv.n_connections)}
+    dtypes = {"<f8": torch.float64, "<i8": torch.int64, "<i4": torch.int32, "|u1": torch.uint8}
+    out = {}
+    for name, typestr, width, dim in _DEVICE_FIELDS:
+        ptr = getattr(dv, name)
+        if not ptr:
+            continue
+        shape = (rows[dim], width) if width > 1 else (rows[dim],)
+        if rows[dim] == 0:
+            out[name] = torch.zeros(shape, dtype=dtypes[typestr], device=device or "cuda")
+        else:
+            out[name] = torch.as_tensor(_DeviceArray(ptr, shape, typestr), device=device)
+    return out
+
+
 def batch_inputs(jobs):
     """Concatenated generators, concatenated mask (or None) and the mv_job descriptors of a
     sequence of tessellations, each a dict with generators, anchor, width, dimensionality,

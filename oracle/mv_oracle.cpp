@@ -21,6 +21,7 @@
 //   * the order among neighbours at exactly equal f64 squared distance (rstar 0.12 /
 //     std BinaryHeap order); this oracle breaks such ties by (index, shift code).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -881,7 +882,14 @@ struct OrcResult {
   std::vector<int64_t> tet_off, cf_off, fv_off;
   std::vector<double> tet_v;
   std::vector<int32_t> tet_plane, cf_plane, fv;
+  // wall seconds of the build's phases: setup (generators, boundary, grid), the
+  // per-cell loop, flatten + finalize
+  double t_setup = 0.0, t_cells = 0.0, t_finalize = 0.0;
 };
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 enum {
   ORC_FACES_ALL = 1,      // compute_face_integrals (non-symmetric): every valid face
@@ -899,6 +907,7 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
                 const double* width, int dim, int periodic, int nthreads, int flags,
                 double ppc, double r0_factor) {
   OrcResult* R = new OrcResult();
+  const double t0 = now_s();
   R->n = n;
   if (n < 0 || (dim < 1 || dim > 3)) {
     R->status = ERR_ARG;
@@ -936,6 +945,8 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
+  const double t1 = now_s();
+  R->t_setup = t1 - t0;
 #pragma omp parallel
   {
     ConvexCell cell;
@@ -979,6 +990,8 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
   }
   R->status = status;
   R->error_cell = err_cell;
+  const double t2 = now_s();
+  R->t_cells = t2 - t1;
   if (status) return R;
 
   // flatten (voronoi.rs:226) and finalize (voronoi.rs:241-263)
@@ -1027,6 +1040,7 @@ void* orc_build(const double* xyz, int64_t n, const uint8_t* mask, const double*
     R->conn.reserve(off);
     for (auto& l : lists) R->conn.insert(R->conn.end(), l.begin(), l.end());
   }
+  R->t_finalize = now_s() - t2;
   if (export_cells) {
     R->pl_off.assign(n + 1, 0), R->vx_off.assign(n + 1, 0);
     for (int64_t k = 0; k < n; k++) {
@@ -1087,6 +1101,10 @@ void orc_copy_face_lists(void* h, int64_t* cf_off, int32_t* cf_plane, int64_t* f
 }
 
 int orc_status(void* h) { return ((OrcResult*)h)->status; }
+void orc_times(void* h, double* out) {
+  const OrcResult* R = (const OrcResult*)h;
+  out[0] = R->t_setup, out[1] = R->t_cells, out[2] = R->t_finalize;
+}
 int64_t orc_error_cell(void* h) { return ((OrcResult*)h)->error_cell; }
 int64_t orc_n_faces(void* h) { return (int64_t)((OrcResult*)h)->f_left.size(); }
 int64_t orc_n_conn(void* h) { return (int64_t)((OrcResult*)h)->conn.size(); }

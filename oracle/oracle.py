@@ -50,6 +50,7 @@ def lib():
         L.orc_copy_faces.argtypes = [P, lp, lp, dp, dp, dp, ip]
         L.orc_copy_conn.argtypes = [P, lp]
         L.orc_copy_stats.argtypes = [P, ip]
+        L.orc_times.argtypes = [P, dp]
         L.orc_copy_cells_export.argtypes = [P, lp, dp, dp, lp, ip, lp, dp, ip]
         for name in ("orc_n_tets_total", "orc_n_cell_faces_total", "orc_n_face_vertices_total"):
             getattr(L, name).restype = C.c_int64
@@ -115,6 +116,8 @@ class OracleVoronoi:
     cell_face_connections: np.ndarray = None
     stats: np.ndarray = None
     cells_export: dict = field(default=None)
+    # wall seconds: setup (generators, boundary, grid), the per-cell loop, finalize
+    times: tuple = (0.0, 0.0, 0.0)
 
 
 def build(generators, anchor, width, dim=3, periodic=False, mask=None, nthreads=0, flags=0,
@@ -136,6 +139,9 @@ def build(generators, anchor, width, dim=3, periodic=False, mask=None, nthreads=
         stats = np.zeros((n, len(STAT_FIELDS)), dtype=np.int32)
         L.orc_copy_stats(h, _ip(stats))
         out.stats = stats
+        tt = np.zeros(3)
+        L.orc_times(h, _dp(tt))
+        out.times = tuple(float(x) for x in tt)
         if st != 0:
             return out
         F = L.orc_n_faces(h)

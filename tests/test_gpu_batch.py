@@ -8,7 +8,7 @@ import pytest
 import meshless_voro_b200 as mv
 from meshless_voro_b200 import workloads as W
 from meshless_voro_b200._native import MV_FACES_ALL, MV_FACES_OWNED, MvError
-from test_gpu_parity import compare
+from voronoi_checks import compare
 
 pytestmark = pytest.mark.gpu
 

@@ -16,11 +16,10 @@ import pytest
 import meshless_voro_b200 as mv
 from meshless_voro_b200 import workloads as W
 from meshless_voro_b200._native import MV_FACES_ALL, MV_FACES_OWNED, MvError
-from voronoi_checks import consistency_check
+from voronoi_checks import REL_TOL, compare, consistency_check  # noqa: F401
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
-REL_TOL = 1e-12
 
 
 def _case(name):
@@ -87,40 +86,6 @@ CASES = ["single", "two", "five_2d", "four_2d_periodic", "lattice4_rect", "latti
          "small_periodic_17", "plane25_periodic_2d", "poisson_2d_rect", "line_1d_periodic",
          "non_perturbed_z", "degenerate_2e15", "clustered30k_periodic", "clustered20k_rect",
          "clustered_2d_periodic", "clump6k_in_3k_periodic"]
-
-
-def _rel_err(a, b, scale):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
-    if a.size == 0:
-        return 0.0
-    return float(np.max(np.abs(a - b) / (np.abs(b) + scale)))
-
-
-def compare(gpu, orc, faces_all=False):
-    """Topology identical, floats within REL_TOL; returns True when bit-identical."""
-    assert orc.status == 0
-    n = len(orc.volume)
-    assert np.array_equal(gpu.face_left, orc.face_left)
-    assert np.array_equal(gpu.face_right, orc.face_right)
-    assert np.array_equal(gpu.face_shift_code, orc.face_shift_code)
-    if not faces_all:
-        assert np.array_equal(gpu.cell_face_offset, orc.face_offset)
-        assert np.array_equal(gpu.cell_face_count, orc.face_count)
-        assert np.array_equal(gpu.cell_face_connections, orc.cell_face_connections)
-    vscale = float(np.max(np.abs(orc.volume))) if n else 1.0
-    lscale = vscale ** (1.0 / 3.0) if vscale > 0 else 1.0
-    assert _rel_err(gpu.cell_volume, orc.volume, 1e-300) <= REL_TOL
-    assert _rel_err(gpu.cell_centroid, orc.centroid, lscale) <= REL_TOL
-    assert _rel_err(gpu.cell_safety_radius, orc.safety_radius, 1e-300) <= REL_TOL
-    ascale = float(np.max(np.abs(orc.face_area))) if len(orc.face_area) else 1.0
-    assert _rel_err(gpu.face_area, orc.face_area, ascale * 1e-6) <= REL_TOL
-    assert _rel_err(gpu.face_centroid, orc.face_centroid, lscale) <= REL_TOL
-    assert np.array_equal(gpu.face_normal, orc.face_normal)
-    return (np.array_equal(gpu.cell_volume, orc.volume)
-            and np.array_equal(gpu.cell_centroid, orc.centroid)
-            and np.array_equal(gpu.face_area, orc.face_area)
-            and np.array_equal(gpu.face_centroid, orc.face_centroid))
 
 
 # the staged pipeline runs in small chunks so that every case spans several of them
