@@ -305,12 +305,14 @@ int mv_context_build_batch(mv_context* ctx, const double* generators, const uint
  * device synchronisation of cudaMalloc/cudaFree, or an embedding with a fixed memory
  * plan.  Same result as mv_context_build_device, on the current device, but every
  * scratch buffer lives in one fixed static device array inside the library, so the
- * call allocates nothing.  That array (about 30 MB) is held by every GPU that loads
+ * call allocates nothing.  That array (about 51 MB) is held by every GPU that loads
  * the library until the process exits.
  *
  * Limits: at most MV_NOALLOC_MAX_GENERATORS generators (larger n returns
  * MV_ERR_CAPACITY without touching the GPU) and at most
- * MV_NOALLOC_FACES_PER_GENERATOR * MV_NOALLOC_MAX_GENERATORS staged faces.
+ * MV_NOALLOC_FACES_PER_GENERATOR * MV_NOALLOC_MAX_GENERATORS staged faces (room for
+ * MV_FACES_ALL on 3-D sets of the full size, about 15.5 faces per cell; a set that
+ * needs more returns MV_ERR_CAPACITY with out->n_faces above that limit).
  *
  * The caller passes device inputs and fills `out` with device pointers sized for n
  * cells (cell_volume, cell_centroid, cell_safety_radius, and for MV_FACES_OWNED
@@ -318,7 +320,9 @@ int mv_context_build_batch(mv_context* ctx, const double* generators, const uint
  * and connection_capacity connections (cell_face_connections, MV_FACES_OWNED only).
  * On return out->n_faces / out->n_connections hold the sizes the build needed; when
  * they exceed the capacities the call returns MV_ERR_CAPACITY.  Runs on opts->stream
- * (NULL: the legacy default stream) and returns when the result is complete.
+ * (NULL: the legacy default stream) and returns when the result is complete.  Cells
+ * whose neighbour shells hold thousands of candidates (the surface of a dense clump)
+ * are built by a few warps only, so such inputs run slower than in a context build.
  *
  * The first call on a device looks up the array's device address (once per device);
  * make that first call before any stream capture.  All calls share the array and it
@@ -326,7 +330,7 @@ int mv_context_build_batch(mv_context* ctx, const double* generators, const uint
  * calls that overlap on the GPU -- from several host threads or streams -- race on it
  * and must be serialised by the caller. */
 #define MV_NOALLOC_MAX_GENERATORS 32768
-#define MV_NOALLOC_FACES_PER_GENERATOR 12
+#define MV_NOALLOC_FACES_PER_GENERATOR 18
 int mv_voronoi_build_noalloc(const double* d_generators, const uint8_t* d_mask, int64_t n,
                              const double anchor[3], const double width[3], int dimensionality,
                              int periodic, const mv_options* opts, mv_device_voronoi* out,

@@ -13,6 +13,12 @@
 // array, and it keeps the contents of the last call: each call clears what must start
 // at zero, and calls that overlap on the GPU (different streams or host threads) race
 // on it.
+//
+// Compared with a context build, the fused kernel's fast tier runs without staging
+// slots for very large neighbour shells (a cell whose shell does not narrow into shared
+// memory moves to the large tier), and the large tier runs on NA_BIG_SLOTS warps, each
+// with one slot inside the array, so it takes the same shells as a context build's
+// large tier.  Results are the same; only such cells take longer.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +27,7 @@
 #include <mutex>
 
 #include "../../include/mvgpu.h"
+#include "mv_cell_common.cuh"
 #include "mv_internal.h"
 
 namespace mv {
@@ -49,6 +56,7 @@ constexpr int64_t NMAX = MV_NOALLOC_MAX_GENERATORS;
 constexpr int64_t CELLMAX = 2 * NMAX;                    // uniform-grid cells
 constexpr int64_t FACEMAX = MV_NOALLOC_FACES_PER_GENERATOR * NMAX;  // staged faces
 constexpr int64_t SCANMAX = (std::max(CELLMAX + 1, NMAX + 1) + 4095) / 4096 + 64;
+constexpr int NA_BIG_SLOTS = 8;  // large-tier warps, one big-shell staging slot each
 
 constexpr size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -77,7 +85,8 @@ constexpr size_t O_STAREA = O_STRIGHT + al(4 * FACEMAX);
 constexpr size_t O_STCEN = O_STAREA + al(8 * FACEMAX);
 constexpr size_t O_STNRM = O_STCEN + al(24 * FACEMAX);
 constexpr size_t O_STCODE = O_STNRM + al(24 * FACEMAX);
-constexpr size_t O_COUNTERS = O_STCODE + al(FACEMAX);
+constexpr size_t O_BIG = O_STCODE + al(FACEMAX);
+constexpr size_t O_COUNTERS = O_BIG + al(NA_BIG_SLOTS * BIG_SLOT_BYTES);
 constexpr size_t SCRATCH_BYTES = O_COUNTERS + al(sizeof(DevCounters));
 
 // The scratch of every no-alloc build on this GPU.  Host code must not use this name
@@ -262,7 +271,9 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
     L.work_counter = &C->work[1];
     L.ovf_list = at<int32_t>(B, O_OVFB);
     L.ovf_count = &C->ovf_count[1];
-    const int blocks = std::min<int>(ds->sm_count * std::max(1, ds->bps_large[pi]), L.n_order);
+    // one warp per block: block b stages its big shells in slot b
+    L.big = reinterpret_cast<char*>(B + O_BIG);
+    const int blocks = std::min<int>(NA_BIG_SLOTS, L.n_order);
     NA_CUDA(launch_cells(L, true, blocks, st, JobTable{nullptr, nullptr, 0}));
     NA_CUDA(cudaMemcpyAsync(&hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
     NA_CUDA(cudaStreamSynchronize(st));
@@ -271,9 +282,10 @@ extern "C" int mv_voronoi_build_noalloc(const double* d_generators, const uint8_
     out->error_cell = hc.status[STATUS_CELL];
     return hc.status[STATUS_CODE];
   }
-  if (hc.ovf_count[1] > 0 || hc.status[STATUS_FACE_OVERFLOW]) return MV_ERR_CAPACITY;
+  // the faces the build asked for (also when they outgrew the staging scratch)
   const int64_t F = (int64_t)hc.face_counter;
   out->n_faces = F;
+  if (hc.ovf_count[1] > 0 || hc.status[STATUS_FACE_OVERFLOW]) return MV_ERR_CAPACITY;
   if (F > face_capacity) return MV_ERR_CAPACITY;
 
   // faces in the reference's order, into the caller's arrays
