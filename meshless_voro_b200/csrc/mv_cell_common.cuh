@@ -892,6 +892,96 @@ __device__ __noinline__ int ring_serial(SM& S, int nvf, int nv, int np) {
   return len;
 }
 
+// The same replay of compute_boundary + SimpleCycle with the whole warp: step i of the
+// reference's loop takes the first removed vertex at or after position i whose dual
+// triangle extends the cycle (failed try_extend calls change nothing), so one ballot
+// over the candidates, 32 at a time, finds it; the rotation / case order of try_extend
+// is kept per candidate.  The cycle's successor pointers end in S.rptr and its
+// iteration order in (S.ea, S.eb); returns the edge count, -1 on failure, -2 when the
+// ring exceeds the tier's vertex capacity.
+template <class T, class SM>
+__device__ __noinline__ int ring_replay_warp(SM& S, int lane, int nvf, int nv, int np) {
+  using PIdx = typename T::PIdx;
+  for (int i = lane; i < np; i += 32) S.rptr[i] = (PIdx)i;
+  __syncwarp();
+  const int s0 = S.ord[nvf];
+  int start = S.vd0[s0];
+  int len = 3;
+  if (lane == 0) {
+    const int a = S.vd0[s0], b = S.vd1[s0], c = S.vd2[s0];
+    S.rptr[a] = (PIdx)b;
+    S.rptr[b] = (PIdx)c;
+    S.rptr[c] = (PIdx)a;
+  }
+  __syncwarp();
+  const int n = nv - nvf;
+  for (int i = 1; i < n; i++) {
+    int found = -1, how = 0;
+    for (int base = i; base < n && found < 0; base += 32) {
+      const int idx = base + lane;
+      int code = 0;  // 1 + 2 * rotation + case (0: grow the cycle, 1: absorb a node)
+      if (idx < n) {
+        const int sl = S.ord[nvf + idx];
+        const int t[3] = {S.vd0[sl], S.vd1[sl], S.vd2[sl]};
+        const bool in[3] = {S.rptr[t[0]] != (PIdx)t[0], S.rptr[t[1]] != (PIdx)t[1],
+                            S.rptr[t[2]] != (PIdx)t[2]};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          const int j = a == 2 ? 0 : a + 1, k = a == 0 ? 2 : a - 1;
+          if (code == 0) {
+            if (!in[a] && in[j] && in[k] && S.rptr[t[k]] == (PIdx)t[j])
+              code = 1 + 2 * a;
+            else if (in[a] && in[j] && in[k] && S.rptr[t[k]] == (PIdx)t[j] &&
+                     S.rptr[t[j]] == (PIdx)t[a])
+              code = 2 + 2 * a;
+          }
+        }
+      }
+      const unsigned bal = __ballot_sync(FULL, code != 0);
+      if (bal) {
+        const int src = __ffs(bal) - 1;
+        found = base + src;
+        how = __shfl_sync(FULL, code, src);
+      }
+    }
+    if (found < 0) return -1;
+    const int sl = S.ord[nvf + found];
+    const int t[3] = {S.vd0[sl], S.vd1[sl], S.vd2[sl]};
+    const int a = (how - 1) >> 1;
+    const int ta = t[a], tb = t[a == 2 ? 0 : a + 1], tc = t[a == 0 ? 2 : a - 1];
+    const bool grow = ((how - 1) & 1) == 0;
+    __syncwarp();
+    if (lane == 0) {
+      S.rptr[tc] = (PIdx)ta;
+      S.rptr[grow ? ta : tb] = (PIdx)tb;
+      if (found > i) {
+        const PIdx tmp = S.ord[nvf + i];
+        S.ord[nvf + i] = S.ord[nvf + found];
+        S.ord[nvf + found] = tmp;
+      }
+    }
+    if (grow) {
+      len += 1;
+    } else {
+      if (start == tb) start = ta;
+      len -= 1;
+    }
+    __syncwarp();
+  }
+  if (len > T::VMAX) return -2;
+  if (lane == 0) {
+    int cur = start;
+    for (int e = 0; e < len; e++) {
+      const int nxt = S.rptr[cur];
+      S.ea[e] = (PIdx)cur;
+      S.eb[e] = (PIdx)nxt;
+      cur = nxt;
+    }
+  }
+  __syncwarp();
+  return len;
+}
+
 // Parallel ring: the boundary edges of the union of the removed dual triangles form
 // the same cycle the serial algorithm builds; it starts at the first removed
 // vertex's dual[0] whenever that node is still on the boundary.  Returns the edge

@@ -414,10 +414,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
         int E = ring_parallel<T>(S, lane, nvf, nv);
         if (E < 0) {
           WCNT(cc, ST_SERIAL_RING, 1);
-          int e2 = 0;
-          if (lane == 0) e2 = ring_serial<T>(S, nvf, nv, np);
-          E = __shfl_sync(FULL, e2, 0);
-          __syncwarp();
+          E = ring_replay_warp<T>(S, lane, nvf, nv, np);
           if (E == -2) return CELL_OVERFLOW;
           if (E < 0) {
             *err_code = MV_ERR_RING;
