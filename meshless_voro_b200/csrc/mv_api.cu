@@ -41,6 +41,9 @@ cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, const Job
 int stage_blocks_per_sm(int kernel, int precision);
 int stage_list_stride();
 int stage_wide_stride();
+cudaError_t launch_append_range(int32_t* dst, int32_t first, int32_t count, cudaStream_t st);
+// cells of the probe chunk that decides between the staged and the fused pipeline
+constexpr int64_t STAGE_PROBE_CELLS = 16384;
 int64_t stage_record_words(int np, int nv);
 // mv_grid.cu
 void launch_prep(const double* xyz, int n, int dim, double* gen, unsigned long long* ext_keys,
@@ -302,7 +305,19 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   // fused kernel shares (keep_records)
   const int64_t chunk = keep_records ? n
                                      : std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
-  const int64_t nchunks = (n + chunk - 1) / chunk;
+  // chunks (first item, items); with the automatic pipeline a small probe chunk comes
+  // first: when most of its cells need the exact predicate (an exact lattice: every
+  // vertex is shared by co-spherical generators) the staged kernels would only hand
+  // the remaining cells on as well, so they go to the fused kernel directly
+  const bool probe = !keep_records && o.pipeline == MV_PIPELINE_AUTO && n >= 4 * STAGE_PROBE_CELLS &&
+                     chunk > STAGE_PROBE_CELLS;
+  std::vector<std::pair<int64_t, int64_t>> chunks;
+  for (int64_t p0 = 0; p0 < n;) {
+    const int64_t m = (probe && p0 == 0) ? STAGE_PROBE_CELLS : std::min<int64_t>(chunk, n - p0);
+    chunks.push_back({p0, m});
+    p0 += m;
+  }
+  const int64_t nchunks = (int64_t)chunks.size();
   const int stride = stage_list_stride();
   int64_t wpc = std::max<int64_t>(record_words_per_cell(dim), (int64_t)ctx->rec_words_hint);
   wpc = std::min<int64_t>(wpc, stage_record_words(64, 64));
@@ -347,8 +362,8 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   SJ.fused_list = keep_records ? SJ.retry_list : P<int32_t>(W.retry2);
   SJ.fused_count = keep_records ? SJ.retry_count : reinterpret_cast<unsigned int*>(ctr + ctr2);
   for (int64_t c = 0; c < nchunks; c++) {
-    SJ.item0 = (int32_t)(c * chunk);
-    SJ.nitems = (int32_t)std::min<int64_t>(chunk, n - c * chunk);
+    SJ.item0 = (int32_t)chunks[c].first;
+    SJ.nitems = (int32_t)chunks[c].second;
     SJ.work = reinterpret_cast<unsigned int*>(ctr + 1 + 3 * c);
     SJ.rec_counter = keep_records ? keep_records : ctr + 1 + 3 * c + 2;
     const int64_t warps_needed = SJ.nitems;
@@ -361,6 +376,33 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
       (*launches)++;
     }
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
+    if (probe && c == 0) {
+      unsigned long long pc[2] = {0, 0};
+      MV_CUDA(cudaMemcpyAsync(&pc[0], ctr, 8, cudaMemcpyDeviceToHost, st));
+      MV_CUDA(cudaMemcpyAsync(&pc[1], ctr + ctr2, 8, cudaMemcpyDeviceToHost, st));
+      MV_CUDA(cudaStreamSynchronize(st));
+      const int64_t n_exact = (int64_t)(pc[1] & 0xffffffffull);
+      if (2 * n_exact >= SJ.nitems) {
+        // the fused kernel's list: the probe's exact cells, its retries, then every
+        // cell after the probe
+        const int64_t n_ret = (int64_t)(pc[0] & 0xffffffffull);
+        int32_t* fl = P<int32_t>(W.retry2);
+        if (n_ret > 0)
+          MV_CUDA(cudaMemcpyAsync(fl + n_exact, P<int32_t>(W.retry), 4 * (size_t)n_ret,
+                                  cudaMemcpyDeviceToDevice, st));
+        MV_CUDA(launch_append_range(fl + n_exact + n_ret, (int32_t)SJ.nitems, (int32_t)(n - SJ.nitems), st));
+        (*launches)++;
+        for (int k = 0; k < 3; k++) {
+          float t = 0.f;
+          cudaEventElapsedTime(&t, ctx->stage_ev[k], ctx->stage_ev[k + 1]);
+          ms_stage[k] = t;
+        }
+        *n_retry = n_exact + n_ret + (n - SJ.nitems);
+        *n_wide = 0;
+        *retry_order = fl;
+        return MV_OK;
+      }
+    }
   }
   std::vector<unsigned long long> h(ctr_words);
   MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * (ctr2 + 1), cudaMemcpyDeviceToHost, st));
@@ -427,7 +469,7 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   // size the record buffer of the next build by what this one asked for
   double need = 0.0;
   for (int64_t c = 0; c < nchunks; c++) {
-    const int64_t items = std::min<int64_t>(chunk, n - c * chunk);
+    const int64_t items = chunks[c].second;
     need = std::max(need, (double)h[1 + 3 * c + 2] / (double)std::max<int64_t>(items, 1));
   }
   if (!keep_records && need * 1.1 > (double)wpc) ctx->rec_words_hint = need * 1.2;

@@ -662,6 +662,18 @@ int stage_blocks_per_sm(int kernel, int precision) {
   return occupancy(integrate_kernel<TierClip, INT_WARPS, false>, 32 * INT_WARPS, 0);
 }
 
+__global__ void append_range_kernel(int32_t* dst, int32_t first, int32_t count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) dst[i] = first + i;
+}
+
+// dst[i] = first + i for i < count (processing positions handed to the fused kernel)
+cudaError_t launch_append_range(int32_t* dst, int32_t first, int32_t count, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  append_range_kernel<<<(count + 255) / 256, 256, 0, st>>>(dst, first, count);
+  return cudaGetLastError();
+}
+
 int stage_list_stride() { return SHELL_CMAX; }
 int stage_wide_stride() { return WIDE_CMAX; }
 
