@@ -298,6 +298,38 @@ int mv_context_build_batch(mv_context* ctx, const double* generators, const uint
                            const mv_job* jobs, int64_t n_jobs, const mv_options* opts,
                            mv_batch_voronoi* out);
 
+/* ---- launch tuning (no counterpart in the reference crate) ----
+ *
+ * The reference builds every cell the same way (voronoi.rs:265-315); this library has
+ * launch parameters whose best values depend on the dimensionality and the size of a
+ * build: the pipeline, the first neighbour shell's radius (initial_radius, in mean
+ * generator spacings: how many neighbours are set up first), the uniform grid's
+ * resolution (points_per_grid_cell) and the staged pipeline's chunk.  The library's
+ * autotuner (meshless_voro_b200/autotune.py) measures them on a B200 per
+ * dimensionality and size band; its table is built into the library.  A build takes
+ * every parameter that its mv_options leave at the default (MV_PIPELINE_AUTO, 0) from
+ * the entry whose band [n_min, n_max) holds its generator count.  Results never depend
+ * on these parameters, only the time does. */
+typedef struct mv_tuning_entry {
+  int32_t dimensionality;        /* 1, 2 or 3                                        */
+  int32_t pipeline;              /* MV_PIPELINE_STAGED or MV_PIPELINE_FUSED          */
+  int64_t n_min, n_max;          /* generator counts n_min <= n < n_max              */
+  double initial_radius;         /* first neighbour shell, in mean spacings          */
+  double points_per_grid_cell;   /* uniform grid resolution                          */
+  int32_t chunk_cells;           /* staged pipeline: cells per chunk                 */
+  int32_t reserved;
+} mv_tuning_entry;
+
+/* Replaces the process-wide table (count == 0: back to the built-in one); returns
+ * MV_ERR_ARG for an invalid entry (and keeps the table). */
+int mv_tuning_set(const mv_tuning_entry* entries, int count);
+
+/* The entry a build of n generators in `dimensionality` dimensions uses. */
+int mv_tuning_lookup(int dimensionality, int64_t n, mv_tuning_entry* out);
+
+/* Entries in the current table. */
+int mv_tuning_count(void);
+
 /* ---- build without allocating (no counterpart in the reference crate) ----
  *
  * For callers that cannot call cudaMalloc -- a host framework that has handed all

@@ -43,6 +43,7 @@ EXPORTED = (
     "mv_context_build", "mv_voronoi_build", "mv_voronoi_build_partial", "mv_voronoi_free",
     "mv_shift_from_code", "mv_voronoi_build_noalloc", "mv_context_build_cells_device",
     "mv_context_build_cells", "mv_context_build_batch_device", "mv_context_build_batch",
+    "mv_tuning_set", "mv_tuning_lookup", "mv_tuning_count",
 )
 
 
@@ -111,6 +112,14 @@ class Job(C.Structure):
     """mv_job: one tessellation of a batch (its rows of the concatenated inputs)."""
     _fields_ = [("n", C.c_int64), ("anchor", C.c_double * 3), ("width", C.c_double * 3),
                 ("dimensionality", C.c_int32), ("periodic", C.c_int32), ("has_mask", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class TuningEntry(C.Structure):
+    """mv_tuning_entry: the launch parameters of one dimensionality and size band."""
+    _fields_ = [("dimensionality", C.c_int32), ("pipeline", C.c_int32), ("n_min", C.c_int64),
+                ("n_max", C.c_int64), ("initial_radius", C.c_double),
+                ("points_per_grid_cell", C.c_double), ("chunk_cells", C.c_int32),
                 ("reserved", C.c_int32)]
 
 
@@ -190,6 +199,12 @@ def lib():
             C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Job), C.c_int64, C.POINTER(Options),
             C.POINTER(BatchVoronoi)]
         L.mv_context_build_batch.restype = C.c_int
+        L.mv_tuning_set.argtypes = [C.POINTER(TuningEntry), C.c_int]
+        L.mv_tuning_set.restype = C.c_int
+        L.mv_tuning_lookup.argtypes = [C.c_int, C.c_int64, C.POINTER(TuningEntry)]
+        L.mv_tuning_lookup.restype = C.c_int
+        L.mv_tuning_count.argtypes = []
+        L.mv_tuning_count.restype = C.c_int
         _lib = L
     return _lib
 

@@ -20,8 +20,9 @@ LIB_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(LIB_DIR, "obj")
 LIB = os.path.join(LIB_DIR, "libmvgpu.so")
 
-SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu", "mv_staged.cu", "mv_export.cu"]
-HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h", "mv_cell_common.cuh"]
+SOURCES = ["mv_api.cu", "mv_cells.cu", "mv_grid.cu", "mv_noalloc.cu", "mv_staged.cu", "mv_export.cu",
+           "mv_tuning.cu"]
+HEADERS = ["mv_geom.cuh", "mv_exact.cuh", "mv_internal.h", "mv_cell_common.cuh", "mv_tuning_table.h"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

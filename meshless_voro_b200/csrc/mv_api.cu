@@ -35,6 +35,8 @@ void launch_export_write(const Job& J, const int64_t* rec_by_orig, const double*
                          double* vert_loc, int32_t* vert_dual, double* tet_v, int32_t* tet_plane,
                          int32_t* face_plane, int64_t* face_vert_off, int32_t* face_verts,
                          int64_t n_faces, int64_t n_face_verts, int32_t* status, cudaStream_t st);
+// mv_tuning.cu
+mv_tuning_entry tuned_params(int dim, int64_t n);
 // mv_staged.cu
 cudaError_t launch_stage(int kernel, const Job& J, const StageJob& SJ, const JobTable& TB, int blocks,
                          cudaStream_t st);
@@ -140,11 +142,13 @@ int make_setup(int64_t n, const double* anchor, const double* width, int dim, in
   s->iloc_inv[0] = 1.0 / (3.0 * bw.x);
   s->iloc_inv[1] = 1.0 / (3.0 * bw.y);
   s->iloc_inv[2] = 1.0 / (3.0 * bw.z);
+  // parameters the options leave to the library: the tuning table's entry
+  const mv_tuning_entry tune = tuned_params(dim, n);
   // uniform grid: ~points_per_grid_cell generators per cell, at most 2^24 cells
   double vol = 1.0;
   for (int i = 0; i < dim; i++) vol *= ww[i];
   const double nn = (double)std::max<int64_t>(n, 1);
-  double ppc = o.points_per_grid_cell > 0 ? o.points_per_grid_cell : 2.2;
+  double ppc = o.points_per_grid_cell > 0 ? o.points_per_grid_cell : tune.points_per_grid_cell;
   double h = std::pow(vol * ppc / nn, 1.0 / dim);
   for (;;) {
     int64_t cells = 1;
@@ -163,7 +167,7 @@ int make_setup(int64_t n, const double* anchor, const double* width, int dim, in
     s->geps[i] = 1e-9 * s->gh[i] + 1e-13 * (std::fabs(aa[i]) + ww[i]);
   }
   const double spacing = std::pow(vol / nn, 1.0 / dim);
-  const double r0 = o.initial_radius > 0 ? o.initial_radius : (dim == 3 ? 2.8 : (dim == 2 ? 2.4 : 2.2));
+  const double r0 = o.initial_radius > 0 ? o.initial_radius : tune.initial_radius;
   s->R0 = r0 * spacing;
   return MV_OK;
 }
@@ -282,13 +286,14 @@ double face_ratio(int dim, int face_mode) {
   return 2.5;
 }
 
-// The staged pipeline runs for builds large enough to fill the GPU with chunks; the
-// candidate list packs a sorted position with a shift code into 32 bits.
-bool use_staged(const mv_options& o, int64_t n) {
+// The automatic pipeline is the tuning table's for the build's band (staged for builds
+// large enough to fill the GPU with chunks); the candidate list packs a sorted
+// position with a shift code into 32 bits.
+bool use_staged(const mv_options& o, int64_t n, int dim) {
   if (n <= 0 || n >= (int64_t)(0xffffffffu / 27u)) return false;
   if (o.pipeline == MV_PIPELINE_STAGED) return true;
   if (o.pipeline == MV_PIPELINE_FUSED) return false;
-  return n >= 65536;
+  return tuned_params(dim, n).pipeline == MV_PIPELINE_STAGED;
 }
 
 int64_t record_words_per_cell(int dim) { return dim == 3 ? 352 : (dim == 2 ? 224 : 128); }
@@ -304,7 +309,8 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   // an export build keeps every cell's record: one chunk, and the record counter the
   // fused kernel shares (keep_records)
   const int64_t chunk = keep_records ? n
-                                     : std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells : (1 << 20));
+                                     : std::min<int64_t>(n, o.chunk_cells > 0 ? o.chunk_cells
+                                                                              : tuned_params(dim, n).chunk_cells);
   // chunks (first item, items); with the automatic pipeline a small probe chunk comes
   // first: when most of its cells need the exact predicate (an exact lattice: every
   // vertex is shared by co-spherical generators) the staged kernels would only hand
@@ -843,7 +849,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
       if (ensure(ctx, W.big, big_slot_bytes(ctx, pi, n))) return MV_ERR_OOM;
       J.big = static_cast<char*>(W.big.p);
     }
-    const bool staged = use_staged(o, n);
+    const bool staged = use_staged(o, n, s.dim);
     if (exporting) {
       // every built cell leaves a record: the staged clip kernel and the fused kernel
       // (retries, small builds, the large tier) write them to one buffer
