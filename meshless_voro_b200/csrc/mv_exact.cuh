@@ -7,7 +7,9 @@
 // differences have 53 bits, squared norms 106, the 3x3 minors at most 215 and the
 // determinant at most 270 bits: fixed 5 x 64-bit two's-complement limbs (arithmetic
 // mod 2^320) are exact.  The sign of an exact integer is unique, so any exact
-// evaluation order agrees with the reference.
+// evaluation order agrees with the reference.  Five corners of one axis-aligned box
+// (the undecided tests of lattice inputs) are recognised first: their determinant is
+// exactly zero.
 #pragma once
 #include <cstdint>
 
@@ -109,10 +111,31 @@ __device__ __forceinline__ S5 det2_small(int64_t a, int64_t b, const S5& c, cons
   return s5_sub(s5_mul_i64(a, d), s5_mul_i64(b, c));
 }
 
+// True when, on every axis, the five points take at most two values: they are then
+// corners of one axis-aligned box (a flat one when an axis has a single value), so all
+// five lie on the box's circumsphere or in one plane and the in-sphere determinant is
+// exactly zero.  Quantised lattice inputs meet this in every undecided test: each
+// coordinate is quantised on its own, so lattice neighbours stay box corners.
+__device__ __forceinline__ bool box_corners(const int64_t a[3], const int64_t b[3],
+                                            const int64_t c[3], const int64_t d[3],
+                                            const int64_t v[3]) {
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const int64_t p0 = a[i];
+    // the first value other than p0 (p0 itself when there is none)
+    const int64_t p1 = b[i] != p0 ? b[i] : (c[i] != p0 ? c[i] : (d[i] != p0 ? d[i] : v[i]));
+    ok = ok && (b[i] == p0 || b[i] == p1) && (c[i] == p0 || c[i] == p1) &&
+         (d[i] == p0 || d[i] == p1) && (v[i] == p0 || v[i] == p1);
+  }
+  return ok;
+}
+
 // Sign of the exact in-sphere determinant (geometry.rs:271-314).  Returns -1, 0, 1.
 static __device__ __noinline__ int in_sphere_exact_sign(const int64_t a[3], const int64_t b[3],
                                                  const int64_t c[3], const int64_t d[3],
                                                  const int64_t v[3]) {
+  if (box_corners(a, b, c, d, v)) return 0;
   // rows: x, y, z (small, 53-bit) and n (squared norm); columns b, c, d, v
   int64_t X[4], Y[4], Z[4];
   S5 N[4];

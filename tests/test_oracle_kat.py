@@ -220,3 +220,26 @@ def test_duplicate_generators_error(oracle):  # convex_cell.rs:325-342 panics
     g = [[0.2, 0.2, 0.2], [0.7, 0.7, 0.7], [0.2, 0.2, 0.2]]
     r = oracle.build(g, [0, 0, 0], [1, 1, 1])
     assert r.status == 2
+
+
+def test_box_corners_in_sphere_is_exactly_zero(oracle):
+    """The exact predicate's shortcut: any five corners of one axis-aligned box (on
+    each axis at most two of the iloc integers) have an exactly zero in-sphere
+    determinant -- they lie on the box's circumsphere, or in one plane."""
+    rng = np.random.default_rng(77)
+    for _ in range(3000):
+        lo = rng.integers(0, 1 << 51, size=3)
+        hi = lo + rng.integers(0, 1 << 50, size=3) * rng.integers(0, 2, size=3)
+        corners = [[(lo, hi)[(m >> i) & 1][i] for i in range(3)] for m in range(8)]
+        pts = [corners[k] for k in rng.integers(0, 8, size=5)]
+        assert oracle.in_sphere_exact(*pts) == 0.0
+    # and a perturbed corner is (almost always) not
+    nz = 0
+    for _ in range(200):
+        lo = rng.integers(0, 1 << 51, size=3)
+        hi = lo + rng.integers(1, 1 << 50, size=3)
+        corners = [[(lo, hi)[(m >> i) & 1][i] for i in range(3)] for m in range(8)]
+        pts = [corners[k] for k in rng.permutation(8)[:5]]
+        pts[4] = [pts[4][0] + 1, pts[4][1], pts[4][2]]
+        nz += oracle.in_sphere_exact(*pts) != 0.0
+    assert nz > 150
