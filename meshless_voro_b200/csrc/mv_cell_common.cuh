@@ -159,8 +159,9 @@ __device__ __noinline__ int exact_clip(const Job& J, const SM& S, int s, D3 x, D
 }
 
 // Vertex::from_dual (convex_cell.rs:28-48) into slot `slot`; *r2 receives the
-// vertex's squared distance to the generator.
-template <class PIdx, class SM>
+// vertex's squared distance to the generator (kept in S.vr2 when STORE_R2; otherwise
+// vertex_r2 recomputes it).
+template <class PIdx, bool STORE_R2 = true, class SM>
 __device__ __forceinline__ bool make_vertex(SM& S, int slot, int i, int j, int k, D3 x, int dim,
                                             double* r2) {
   D3 loc;
@@ -175,7 +176,7 @@ __device__ __forceinline__ bool make_vertex(SM& S, int slot, int i, int j, int k
   S.vx[slot] = loc.x;
   S.vy[slot] = loc.y;
   S.vz[slot] = loc.z;
-  S.vr2[slot] = rr;
+  if constexpr (STORE_R2) S.vr2[slot] = rr;
   S.f4[slot] = make_float4(__double2float_rn(loc.x - x.x), __double2float_rn(loc.y - x.y),
                            __double2float_rn(loc.z - x.z), 0.f);
   S.vd0[slot] = (PIdx)i;
@@ -183,6 +184,17 @@ __device__ __forceinline__ bool make_vertex(SM& S, int slot, int i, int j, int k
   S.vd2[slot] = (PIdx)k;
   *r2 = rr;
   return true;
+}
+
+// The squared distance of the vertex in slot `slot` to the generator, as make_vertex
+// computes it (Vertex::from_dual, convex_cell.rs:38-42).
+template <class SM>
+__device__ __forceinline__ double vertex_r2(const SM& S, int slot, D3 x, int dim) {
+  D3 dl = {S.vx[slot], S.vy[slot], S.vz[slot]};
+  if (dim == 1) dl = {dl.x, 0.0, 0.0};
+  if (dim == 2) dl = {dl.x, dl.y, 0.0};
+  const D3 r = sub(x, dl);
+  return dot(r, r);
 }
 
 // Vertex duals of the initial cuboid (convex_cell.rs:298-307), one vertex per lane.
@@ -1049,6 +1061,13 @@ __device__ __forceinline__ int ring_parallel(SM& S, int lane, int nvf, int nv) {
 // instead of a walk.  Lane e < E receives edge (*eu -> *ew) at ring position *erank.
 // Returns E, or -1 when the serial replay must decide (the start node is interior,
 // the edges do not form one cycle through it, or more than 32 edges).
+//
+// The boundary test uses S.plm, one 32-bit lane mask per plane (zero between calls):
+// removed triangle `lane` sets its bit on its three planes.  The dual of a convex cell
+// is a triangulated sphere, so an edge {u, w} belongs to exactly two triangles, with
+// opposite orientations; edge u->w of a removed triangle is therefore interior (the
+// other triangle, holding w->u, is removed as well) exactly when another removed
+// triangle holds both u and w.
 template <class T, class SM>
 __device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int* eu, int* ew,
                                            int* erank) {
@@ -1056,26 +1075,28 @@ __device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int
   const int r = nv - nvf;
   if (r > 32) return -1;
   int t0 = 0, t1 = 0, t2 = 0;
+  const unsigned me = 1u << lane;
   if (lane < r) {
     const int sl = S.ord[nvf + lane];
     t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
     S.rptr[t0] = (PIdx)T::NONE;
     S.rptr[t1] = (PIdx)T::NONE;
     S.rptr[t2] = (PIdx)T::NONE;
+    atomicOr(&S.plm[t0], me);
+    atomicOr(&S.plm[t1], me);
+    atomicOr(&S.plm[t2], me);
   }
   const int start = S.vd0[S.ord[nvf]];
   __syncwarp();
-  // an edge u->w of a removed triangle is on the boundary iff no other removed
-  // triangle holds w->u
-  bool b01 = lane < r, b12 = lane < r, b20 = lane < r;
-  for (int k = 0; k < r; k++) {
-    const int a = __shfl_sync(FULL, t0, k), b = __shfl_sync(FULL, t1, k),
-              c = __shfl_sync(FULL, t2, k);
-    if (k == lane) continue;
-    b01 = b01 && !((a == t1 && b == t0) || (b == t1 && c == t0) || (c == t1 && a == t0));
-    b12 = b12 && !((a == t2 && b == t1) || (b == t2 && c == t1) || (c == t2 && a == t1));
-    b20 = b20 && !((a == t0 && b == t2) || (b == t0 && c == t2) || (c == t0 && a == t2));
+  bool b01 = false, b12 = false, b20 = false;
+  if (lane < r) {
+    const unsigned m0 = S.plm[t0] & ~me, m1 = S.plm[t1] & ~me, m2 = S.plm[t2] & ~me;
+    b01 = (m0 & m1) == 0u;
+    b12 = (m1 & m2) == 0u;
+    b20 = (m2 & m0) == 0u;
   }
+  __syncwarp();
+  if (lane < r) S.plm[t0] = 0u, S.plm[t1] = 0u, S.plm[t2] = 0u;
   const unsigned m01 = __ballot_sync(FULL, b01), m12 = __ballot_sync(FULL, b12),
                  m20 = __ballot_sync(FULL, b20);
   const int n01 = __popc(m01), n12 = __popc(m12);

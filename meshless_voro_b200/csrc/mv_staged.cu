@@ -218,8 +218,9 @@ struct ClipSmem {
   uint8_t pcode[T::PMAX];   // periodic shift code, 13: none
   PIdx rptr[T::PMAX];       // ring successor (SimpleCycle::ptrs)
   // vertices (convex_cell.rs:16-25) in fixed slots
-  double vx[T::VMAX], vy[T::VMAX], vz[T::VMAX], vr2[T::VMAX];
+  double vx[T::VMAX], vy[T::VMAX], vz[T::VMAX];
   float4 f4[T::VMAX];  // f32 (v - x) for the filter
+  uint32_t plm[T::PMAX];  // ring_ranked: lanes whose removed triangle holds the plane
   alignas(4) PIdx ord[T::VMAX];   // position -> slot; [0, nv) is the reference's order
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
@@ -270,13 +271,14 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
     S.pcode[lane] = 13;
   }
   for (int i = lane; i < T::VMAX; i += 32) S.ord[i] = (PIdx)i;
+  for (int i = lane; i < T::PMAX; i += 32) S.plm[i] = 0u;
   __syncwarp();
+  double r2init = 0.0;
   {
     int i0 = 0, i1 = 0, i2 = 0;
     cuboid_duals(lane, &i0, &i1, &i2);
     bool ok = true;
-    double r2 = 0.0;
-    if (lane < 8) ok = make_vertex<PIdx>(S, lane, i0, i1, i2, x, dim, &r2);
+    if (lane < 8) ok = make_vertex<PIdx, false>(S, lane, i0, i1, i2, x, dim, &r2init);
     if (__any_sync(FULL, !ok)) {
       *err_code = MV_ERR_DET;
       return CELL_ERROR;
@@ -284,7 +286,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   }
   __syncwarp();
   int nv = 8, np = 6;
-  double max_r2 = warp_max_nonneg(lane < 8 ? S.vr2[lane] : 0.0);
+  double max_r2 = warp_max_nonneg(lane < 8 ? r2init : 0.0);
   double sr = 2.0 * sqrt(max_r2);
   float A32 = amax32_of_sr(sr, dim);
   const double x1 = fabs(x.x) + fabs(x.y) + fabs(x.z);
@@ -441,12 +443,26 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       cc.plane();
 
       // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
-      // over 64-bit masks of removed / kept positions; kept vertices before nvf stay
+      // over 64-bit masks of removed / kept positions; kept vertices before nvf stay.
+      // The s-th removed / kept position comes from inverse maps built in S.ea / S.eb
+      // (free until the ring below).
       const unsigned long long rm64 = ((unsigned long long)rm[1] << 32) | rm[0];
       const unsigned long long km64 = ~rm64 & (nv >= 64 ? ~0ull : ((1ull << nv) - 1ull));
       const int totK = __popcll(km64);
       const int nvf = totK;
       {
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+          const int q = lane + 32 * w;
+          if (q < nv) {
+            const unsigned long long below = (1ull << q) - 1ull;
+            if ((rm64 >> q) & 1ull)
+              S.ea[__popcll(rm64 & below)] = (PIdx)q;
+            else
+              S.eb[__popcll(km64 & below)] = (PIdx)q;
+          }
+        }
+        __syncwarp();
         int dest[2];
         PIdx held[2];
 #pragma unroll
@@ -457,10 +473,10 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           if (q < nv) {
             const unsigned long long below = (1ull << q) - 1ull;
             if (!((rm64 >> q) & 1ull)) {
-              if (q >= nvf) dd = select64(rm64, totK - __popcll(km64 & below));
+              if (q >= nvf) dd = S.ea[totK - __popcll(km64 & below) - 1];
             } else if (q <= nvf) {
               const int t = __popcll(rm64 & below) + 1;
-              dd = ((t == 1) ? nv : select64(km64, totK - t + 2)) - 1;
+              dd = ((t == 1) ? nv : (int)S.eb[totK - t + 1]) - 1;
             } else {
               dd = q - 1;
             }
@@ -495,11 +511,11 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       bool ok = true;
       double r2n = 0.0;
       if (lane < E) {
-        ok = make_vertex<PIdx>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
+        ok = make_vertex<PIdx, false>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
         mk = fmax(mk, r2n);
       }
       for (int ei = lane + 32; ei < E; ei += 32) {  // rings of more than 32 edges (serial replay)
-        ok &= make_vertex<PIdx>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
+        ok &= make_vertex<PIdx, false>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
         mk = fmax(mk, r2n);
       }
       if (__any_sync(FULL, !ok)) {
@@ -510,7 +526,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       nv = nvf + E;
       // update_safety_radius (convex_cell.rs:443-453): the maximum over the kept and the
       // new vertices
-      for (int q = lane; q < nvf; q += 32) mk = fmax(mk, S.vr2[S.ord[q]]);
+      for (int q = lane; q < nvf; q += 32) mk = fmax(mk, vertex_r2(S, S.ord[q], x, dim));
       const double mr = warp_max_nonneg(mk);
       if (__double_as_longlong(mr) != __double_as_longlong(max_r2)) {
         max_r2 = mr;
