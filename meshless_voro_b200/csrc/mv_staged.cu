@@ -224,13 +224,13 @@ struct ClipSmem {
   alignas(4) PIdx ord[T::VMAX];   // position -> slot; [0, nv) is the reference's order
   PIdx vd0[T::VMAX], vd1[T::VMAX], vd2[T::VMAX];
   PIdx ea[T::VMAX], eb[T::VMAX];  // ring edges in SimpleCycle iteration order
-  // the window: 32 consecutive candidates of the list, as the reference sets them up
-  // (location, distance) plus the f32 operands and bound coefficients of the filter
-  double wgx[32], wgy[32], wgz[32], wdist[32];
+  // the window: 32 consecutive candidates of the list with their half-spaces as the
+  // reference sets them up (HalfSpace::new: normal, offset d = n.p, error bound errb),
+  // plus the f32 operands and bound coefficients of the filter
+  double wnx[32], wny[32], wnz[32], wd[32], werr[32];
   float4 wf[32];  // filter operands: e = x - ngb in f32, |e|^2 / 2
   float2 wc[32];  // bound coefficients (c0, c1)
-  int32_t worig[32];
-  uint8_t wcode[32];
+  uint32_t wpk[32];  // original index * 27 + shift code
   __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
   // HalfSpace::p of plane k: the boundary point, or (x + ngb) / 2 recomputed as at the clip
   __device__ D3 bisector_point(const Job& J, int k, D3 x) const {
@@ -302,6 +302,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
     // candidate w0 + lane: location and offset as the reference computes them
     // (convex_cell.rs:333-342), plus the f32 quantities of the filter
     bool bad = false, filt = false;
+    double dist = 0.0;  // this lane's candidate's distance |x - ngb|
     if (valid) {
       const uint32_t pk = __ldg(list + w0 + lane);
       const int cp = (int)(pk / 27u);
@@ -310,11 +311,15 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const int orig = __ldg(J.sid + cp);
       if (code != 13) g = add(g, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
       const D3 dx = sub(x, g);
-      const double dist = sqrt(dot(dx, dx));
+      dist = sqrt(dot(dx, dx));
       bad = !(dist > 0.0 && dist <= DBL_MAX);
-      S.wgx[lane] = g.x, S.wgy[lane] = g.y, S.wgz[lane] = g.z, S.wdist[lane] = dist;
-      S.worig[lane] = orig;
-      S.wcode[lane] = (uint8_t)code;
+      // HalfSpace::new (half_space.rs:24-34) for every candidate of the window at once
+      const D3 n = divs(dx, dist);
+      const D3 p = scale(0.5, add(x, g));
+      S.wnx[lane] = n.x, S.wny[lane] = n.y, S.wnz[lane] = n.z;
+      S.wd[lane] = dot(n, p);
+      S.werr[lane] = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
+      S.wpk[lane] = (uint32_t)orig * 27u + (uint32_t)code;
       if (PREC == MV_PRECISION_FILTERED) {
         // s = e.a + |e|^2 / 2 is certified by T = c0 + c1 A with A >= |v - x| over the
         // cell's vertices (the bound of setup_batch, split into its A-free and A parts)
@@ -336,7 +341,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
     unsigned mfilt = 0u;
     if (PREC == MV_PRECISION_FILTERED) mfilt = __ballot_sync(FULL, valid && filt && A32 <= 1e15f);
     // beyond the safety radius (refreshed when a clip shrinks it)
-    unsigned mstop = __ballot_sync(FULL, valid && !bad && sr < S.wdist[lane]);
+    unsigned mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
     // the f32 offset of this lane's vertex (position lane) for the filter
     float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
     if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
@@ -374,10 +379,6 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const int e = k++;
       cc.neighbours(1);
       // ---- candidate e: HalfSpace::new (half_space.rs:24-34) and clip_by_plane ----
-      const D3 ngb = {S.wgx[e], S.wgy[e], S.wgz[e]};
-      const double de = S.wdist[e];
-      const int orig_e = S.worig[e];
-      const int code_e = S.wcode[e];
       bool filt_e = false;
       float exe = 0.f, eye = 0.f, eze = 0.f, he = 0.f, Tk = 0.f;
       if (PREC == MV_PRECISION_FILTERED) {
@@ -387,11 +388,9 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         exe = fe.x, eye = fe.y, eze = fe.z, he = fe.w;
         Tk = __fmaf_ru(ce.y, A32, ce.x);
       }
-      const D3 dx = sub(x, ngb);
-      const D3 n = divs(dx, de);
-      const D3 p = scale(0.5, add(x, ngb));
-      const double errb = 1e-13 * (1.0 + dot(vabs(n), vabs(p)));
-      const double d = dot(n, p);
+      const D3 n = {S.wnx[e], S.wny[e], S.wnz[e]};
+      const double errb = S.werr[e];
+      const double d = S.wd[e];
       unsigned rm[T::NW];
       int n_und = 0;
       bool need_exact = false;
@@ -434,10 +433,11 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       if (np >= T::PMAX) return CELL_OVERFLOW;
       const int p_idx = np;
       if (lane == 0) {
+        const uint32_t pk = S.wpk[e];
         S.pnx[p_idx] = n.x, S.pny[p_idx] = n.y, S.pnz[p_idx] = n.z;
         S.pd[p_idx] = d;
-        S.pright[p_idx] = orig_e;
-        S.pcode[p_idx] = (uint8_t)code_e;
+        S.pright[p_idx] = (int32_t)(pk / 27u);
+        S.pcode[p_idx] = (uint8_t)(pk % 27u);
       }
       np++;
       cc.plane();
@@ -533,7 +533,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         sr = 2.0 * sqrt(max_r2);
         A32 = amax32_of_sr(sr, dim);
       }
-      mstop = __ballot_sync(FULL, valid && !bad && sr < S.wdist[lane]);
+      mstop = __ballot_sync(FULL, valid && !bad && sr < dist);
       if (PREC == MV_PRECISION_FILTERED && lane < nv) fv = S.f4[S.ord[lane]];
     }
   }
