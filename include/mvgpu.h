@@ -167,7 +167,11 @@ int mv_context_build_device(mv_context* ctx, const double* d_generators, const u
 
 /* Same as mv_context_build_device with host inputs; the result is copied into the
  * context's pinned host arena (valid until the next build on the context).  *out
- * is owned by the context: do not pass it to mv_voronoi_free. */
+ * is owned by the context: do not pass it to mv_voronoi_free.  Builds with host
+ * buffers (this call, mv_context_build_cells and mv_context_build_batch) on one
+ * device run their GPU phase one at a time and copy their results back outside it:
+ * with one context per host thread, one build's result copy overlaps the next
+ * build's kernels. */
 int mv_context_build(mv_context* ctx, const double* generators, const uint8_t* mask, int64_t n,
                      const double anchor[3], const double width[3], int dimensionality,
                      int periodic, const mv_options* opts, mv_voronoi** out);

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1445,6 +1446,26 @@ int copy_cells_to_host(mv_context* ctx, const mv_cells& d, cudaStream_t st, mv_c
   return MV_OK;
 }
 
+// Builds with host buffers run their GPU phase (input copy, kernels) one at a time per
+// device and copy their results back outside it: with several contexts on one device
+// (one per host thread), one build's result copy then overlaps the next build's
+// kernels, instead of all builds computing side by side and copying at once.
+constexpr int MAX_PHASE_DEVICES = 64;
+std::mutex g_gpu_phase[MAX_PHASE_DEVICES];
+
+struct GpuPhase {
+  std::mutex* m;
+  explicit GpuPhase(int device)
+      : m(device >= 0 && device < MAX_PHASE_DEVICES ? &g_gpu_phase[device] : nullptr) {
+    if (m) m->lock();
+  }
+  void release() {
+    if (m) m->unlock();
+    m = nullptr;
+  }
+  ~GpuPhase() { release(); }
+};
+
 int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int64_t n,
                     const double* anchor, const double* width, int dim, int periodic,
                     const mv_options* opts, mv_voronoi** out, int cells_flags = -1,
@@ -1458,6 +1479,7 @@ int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int
   if (rc) return rc;
   MV_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  GpuPhase phase(ctx->device);
   const size_t N = (size_t)std::max<int64_t>(n, 1);
   if (ensure(ctx, ctx->ws.in_xyz, 24 * N) || ensure(ctx, ctx->ws.in_mask, N)) return MV_ERR_OOM;
   if (n > 0) MV_CUDA(cudaMemcpyAsync(ctx->ws.in_xyz.p, xyz, 24 * (size_t)n, cudaMemcpyHostToDevice, st));
@@ -1475,6 +1497,7 @@ int build_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mask, int
     *out = &ctx->hv;
     return rc;
   }
+  phase.release();
   rc = copy_to_host(ctx, d, n, s, st, &ctx->hv);
   if (rc) return rc;
   *out = &ctx->hv;
@@ -1504,6 +1527,7 @@ int build_batch_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mas
   if ((ntot > 0 && !xyz) || (any_mask && !mask)) return MV_ERR_ARG;
   MV_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = o.stream ? (cudaStream_t)o.stream : ctx->stream;
+  GpuPhase phase(ctx->device);
   const size_t N = (size_t)std::max<int64_t>(ntot, 1);
   if (ensure(ctx, ctx->ws.in_xyz, 24 * N) || ensure(ctx, ctx->ws.in_mask, N)) return MV_ERR_OOM;
   if (ntot > 0)
@@ -1520,6 +1544,7 @@ int build_batch_host_impl(mv_context* ctx, const double* xyz, const uint8_t* mas
     *out = d;
     return rc;
   }
+  phase.release();
   HostLayout L = host_layout(d.n_cells, d.n_faces, d.n_connections);
   if (ctx->host_cap < L.total) {
     if (ctx->host) cudaFreeHost(ctx->host);
