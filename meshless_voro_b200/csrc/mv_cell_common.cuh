@@ -1231,33 +1231,36 @@ __device__ __forceinline__ bool line_projection(const View& V, int q, int i, D3 
 }
 
 // --------------------------------------------------------------- integrals --
-// Scratch of the integral step: projections on the plane-pair lines of 5 vertices
-// and the 30 tets' values (rows padded so that lanes reading different rows at the
-// same column hit different banks).
+// Scratch of the integral step: projections on the plane-pair lines of STEP vertices
+// and their 6 STEP tets' values (rows padded so that lanes reading different rows at
+// the same column hit different banks).
+template <int STEP = 5>
 struct TetScratch {
-  double ix[15], iy[15], iz[15];
-  double val[8][33];
+  static constexpr int NT = 6 * STEP;
+  double ix[3 * STEP], iy[3 * STEP], iz[3 * STEP];
+  double val[8][NT + 3];
 };
 
 // Integrals and face emission of a finished cell (convex_cell.rs:131-187,
 // voronoi_cell.rs:40-100) over a view V of the cell: V.normal(pl), V.d(pl),
 // V.proj(pl) (the generator projected on plane pl), V.right(pl), V.code(pl),
 // V.dual(q, i) and V.loc(q) for vertex position q in the reference's order.  Each
-// 5-vertex step projects on the 15 plane-pair lines, builds the 30 tets (one per
-// lane) and accumulates them in the reference's tet order: lanes 0-3 the cell
-// integrals, lane p (and p + 32k) the integrals of face p.
-template <class T, class View>
-__device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetScratch& Sc, int lane,
-                                              int self, D3 x, int nv, int np, double sr,
+// step of STEP vertices (STEP <= 10) projects on their 3 STEP plane-pair lines (one
+// per lane), builds their 6 STEP tets and accumulates them in the reference's tet
+// order: lanes 0-3 the cell integrals, lane p (and p + 32k) the integrals of face p.
+template <class T, int STEP, class View>
+__device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetScratch<STEP>& Sc,
+                                              int lane, int self, D3 x, int nv, int np, double sr,
                                               int* err_code) {
+  static_assert(3 * STEP <= 32, "one projection per lane");
   const int dim = J.dim;
   double cacc = 0.0;  // lanes 0..3: volume, centroid x, y, z
   double fa[T::PMAX / 32], fcx[T::PMAX / 32], fcy[T::PMAX / 32], fcz[T::PMAX / 32];
   unsigned ftouched = 0;
 #pragma unroll
   for (int k = 0; k < T::PMAX / 32; k++) fa[k] = 0.0, fcx[k] = 0.0, fcy[k] = 0.0, fcz[k] = 0.0;
-  for (int base = 0; base < nv; base += 5) {
-    const int nstep = min(5, nv - base);
+  for (int base = 0; base < nv; base += STEP) {
+    const int nstep = min(STEP, nv - base);
     // projections on the lines dual[i] & dual[i+1]: project_onto_intersection
     // (geometry.rs:41-47) of plane dual[(i+1)%3] with dual[i]
     bool ok = true;
@@ -1276,8 +1279,8 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
     __syncwarp();
     // DecompositionWithoutFaces: tet t of a vertex = (proj[t], proj[(t+5)%6], vertex)
     // with proj[2i] on plane dual[i] and proj[2i+1] on the line (dual[i+1], dual[i])
-    if (lane < 6 * nstep) {
-      const int vl = lane / 6, t = lane - 6 * vl;
+    for (int tt = lane; tt < 6 * nstep; tt += 32) {
+      const int vl = tt / 6, t = tt - 6 * vl;
       const int q = base + vl;
       auto proj = [&](int qq) -> D3 {
         const int i = qq >> 1;
@@ -1290,14 +1293,14 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
       const D3 vc = scale(vol, add(add(add(v0, v1), vloc), x));
       const double ar = signed_area_tri(v0, v1, vloc, x);
       const D3 ac = scale(ar, add(add(v0, v1), vloc));
-      Sc.val[0][lane] = vol;
-      Sc.val[1][lane] = vc.x;
-      Sc.val[2][lane] = vc.y;
-      Sc.val[3][lane] = vc.z;
-      Sc.val[4][lane] = ar;
-      Sc.val[5][lane] = ac.x;
-      Sc.val[6][lane] = ac.y;
-      Sc.val[7][lane] = ac.z;
+      Sc.val[0][tt] = vol;
+      Sc.val[1][tt] = vc.x;
+      Sc.val[2][tt] = vc.y;
+      Sc.val[3][tt] = vc.z;
+      Sc.val[4][tt] = ar;
+      Sc.val[5][tt] = ac.x;
+      Sc.val[6][tt] = ac.y;
+      Sc.val[7][tt] = ac.z;
     }
     __syncwarp();
     const int ntet = 6 * nstep;

@@ -75,7 +75,7 @@ struct CellSmem {
     } g;
     struct {  // integration phase
       double px[T::PMAX], py[T::PMAX], pz[T::PMAX];  // generator projected on each plane
-      TetScratch ts;
+      TetScratch<5> ts;
     } t;
   } u;
 };
@@ -113,7 +113,7 @@ __device__ __noinline__ int integrate_cell(const Job& J, CellSmem<T>& S, int lan
   }
   __syncwarp();
   const SmemView<T> V{S};
-  return integrate_view<T>(J, V, S.u.t.ts, lane, self, x, nv, np, sr, err_code);
+  return integrate_view<T, 5>(J, V, S.u.t.ts, lane, self, x, nv, np, sr, err_code);
 }
 
 // Sets up neighbours [j, j + kb) of the sorted shell, one lane each: f64 location,

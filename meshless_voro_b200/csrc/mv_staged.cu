@@ -40,6 +40,10 @@ constexpr int SHELL_WARPS = 4;
 #endif
 constexpr int CLIP_WARPS = MV_CLIP_WARPS;
 constexpr int INT_WARPS = 4;
+#ifndef MV_INT_STEP
+#define MV_INT_STEP 10
+#endif
+constexpr int INT_STEP = MV_INT_STEP;  // vertices per step of the integral kernel
 #ifndef MV_INT_MINB
 #define MV_INT_MINB 8
 #endif
@@ -619,7 +623,7 @@ template <class T, int WARPS, bool MULTI>
 __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB)
     integrate_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
                      const __grid_constant__ JobTable TB) {
-  __shared__ TetScratch scratch[WARPS];
+  __shared__ TetScratch<INT_STEP> scratch[WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned done = 0;
   for (;;) {
@@ -637,7 +641,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB)
     const D3 x = load_gen(J, self);
     const RecordView V(SJ.rec + off);
     int err = 0;
-    const int res = integrate_view<T>(J, V, scratch[warp], lane, self, x, V.nv, V.np, V.sr, &err);
+    const int res = integrate_view<T, INT_STEP>(J, V, scratch[warp], lane, self, x, V.nv, V.np, V.sr, &err);
     if (res == CELL_DONE) {
       done++;
     } else if (lane == 0) {
