@@ -233,7 +233,19 @@ struct mv_context {
   void* host_cells = nullptr;
   size_t host_cells_cap = 0;
   mv_cells hc{};
+  // mapped pinned buffer for the build's small device-to-host reads (readback)
+  void* rb_host = nullptr;
+  void* rb_dev = nullptr;
 };
+
+namespace {
+constexpr size_t READBACK_BYTES = 1 << 20;
+
+__global__ void readback_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, int nwords) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+}  // namespace
 
 namespace {
 
@@ -280,6 +292,33 @@ template <class T>
 T* P(DevBuf& b) {
   return static_cast<T*>(b.p);
 }
+
+// A small device-to-host read inside a build (counters, sizes), complete on return.
+// It goes through a kernel into the context's mapped pinned buffer rather than a
+// cudaMemcpy: a copy would queue on the copy engine behind any bulk result copy that
+// another context has in flight, stalling this build until that copy ends.
+int readback(mv_context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return MV_OK;
+  if (ctx->rb_dev && bytes % 4 == 0 && bytes <= READBACK_BYTES &&
+      reinterpret_cast<uintptr_t>(src) % 4 == 0) {
+    const int nw = (int)(bytes / 4);
+    readback_kernel<<<std::min(64, (nw + 255) / 256), 256, 0, st>>>(
+        static_cast<const uint32_t*>(src), static_cast<uint32_t*>(ctx->rb_dev), nw);
+    MV_CUDA(cudaGetLastError());
+    MV_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(dst, ctx->rb_host, bytes);
+    return MV_OK;
+  }
+  MV_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+  MV_CUDA(cudaStreamSynchronize(st));
+  return MV_OK;
+}
+
+#define MV_RB(dst, src, bytes)                            \
+  do {                                                    \
+    const int rb_ = readback(ctx, (dst), (src), (bytes), st); \
+    if (rb_) return rb_;                                  \
+  } while (0)
 
 double face_ratio(int dim, int face_mode) {
   if (dim == 3) return face_mode == MV_FACES_ALL ? 17.5 : 10.5;
@@ -385,9 +424,8 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
     if (probe && c == 0) {
       unsigned long long pc[2] = {0, 0};
-      MV_CUDA(cudaMemcpyAsync(&pc[0], ctr, 8, cudaMemcpyDeviceToHost, st));
-      MV_CUDA(cudaMemcpyAsync(&pc[1], ctr + ctr2, 8, cudaMemcpyDeviceToHost, st));
-      MV_CUDA(cudaStreamSynchronize(st));
+      MV_RB(&pc[0], ctr, 8);
+      MV_RB(&pc[1], ctr + ctr2, 8);
       const int64_t n_exact = (int64_t)(pc[1] & 0xffffffffull);
       if (2 * n_exact >= SJ.nitems) {
         // the fused kernel's list: the probe's exact cells, its retries, then every
@@ -412,8 +450,7 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
     }
   }
   std::vector<unsigned long long> h(ctr_words);
-  MV_CUDA(cudaMemcpyAsync(h.data(), ctr, 8 * (ctr2 + 1), cudaMemcpyDeviceToHost, st));
-  MV_CUDA(cudaStreamSynchronize(st));
+  MV_RB(h.data(), ctr, 8 * (ctr2 + 1));
   // the first round's retries: for the wide round, or with kept records (one list,
   // exact cells included) for the fused kernel
   const int64_t n_first = (int64_t)(h[0] & 0xffffffffull);
@@ -460,8 +497,7 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
       MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
     }
     unsigned long long r2 = 0;
-    MV_CUDA(cudaMemcpyAsync(&r2, ctr + ctr2, 8, cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
+    MV_RB(&r2, ctr + ctr2, 8);
     for (int64_t c = 0; c < nc; c++) {
       for (int k = 0; k < 3; k++) {
         float t = 0.f;
@@ -579,8 +615,7 @@ int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, c
   stats->ms_clip = ms_stage[1];
   stats->ms_integrate = ms_stage[2];
   bool large_ran = false;
-  MV_CUDA(cudaMemcpyAsync(hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-  MV_CUDA(cudaStreamSynchronize(st));
+  MV_RB(hc, C, sizeof(DevCounters));
   if (hc->bad_input) return MV_ERR_ARG;
   const unsigned novf = hc->ovf_count[0];
   if (novf > 0 && !hc->status[STATUS_CODE]) {
@@ -598,8 +633,7 @@ int run_cell_phase(mv_context* ctx, const Job& J, const JobTable& TB, int dim, c
     MV_CUDA(cudaEventRecord(ctx->ev[4], st));
     (*launches)++;
     large_ran = true;
-    MV_CUDA(cudaMemcpyAsync(hc, C, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
+    MV_RB(hc, C, sizeof(DevCounters));
   }
   ctx->large_ran = large_ran;
   return MV_OK;
@@ -625,7 +659,7 @@ int export_cells(mv_context* ctx, const Job& J, int64_t n, int flags, cudaStream
   if (n > 0) {
     for (int k = 0; k < 5; k++) {
       scan_i32_to_i64(cnt + k * N, n, off + k * (N + 1), P<long long>(W.scan_tmp), st);
-      MV_CUDA(cudaMemcpyAsync(&tot[k], off + k * (N + 1) + n, 8, cudaMemcpyDeviceToHost, st));
+      MV_RB(&tot[k], off + k * (N + 1) + n, 8);
     }
     *launches += 15;
   } else {
@@ -655,8 +689,7 @@ int export_cells(mv_context* ctx, const Job& J, int64_t n, int flags, cudaStream
   *launches += (flags & MV_CELLS_WITH_FACES) ? 2 : 1;
   MV_CUDA(cudaGetLastError());
   int32_t status[STATUS_WORDS];
-  MV_CUDA(cudaMemcpyAsync(status, C->status, sizeof(status), cudaMemcpyDeviceToHost, st));
-  MV_CUDA(cudaStreamSynchronize(st));
+  MV_RB(status, C->status, sizeof(status));
   if (status[STATUS_CODE]) return status[STATUS_CODE];
   std::memset(out, 0, sizeof(*out));
   out->n_cells = n;
@@ -778,8 +811,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
                        P<int32_t>(W.cell_count), P<int32_t>(W.cell_start), P<int32_t>(W.dflag),
                        P<int32_t>(W.dprefix), s.dim, P<long long>(W.scan_tmp), st);
     int32_t ndense = 0;
-    MV_CUDA(cudaMemcpyAsync(&ndense, P<int32_t>(W.dprefix) + ncell, 4, cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
+    MV_RB(&ndense, P<int32_t>(W.dprefix) + ncell, 4);
     if (ndense > 0) {
       // clustered input: the dense cells are ordered by Morton key (a radix sort)
       const size_t sort_bytes = grid_dense_sort_bytes(ni, ncell);
@@ -929,8 +961,7 @@ int build_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t* d_mas
     launch_csr_counts(fin, F, P<int32_t>(W.face_count), ni, P<int32_t>(W.in_count),
                       P<int32_t>(W.conn_count), st);
     scan_i32_to_i64(P<int32_t>(W.conn_count), n, P<int64_t>(W.conn_off), P<long long>(W.scan_tmp), st);
-    MV_CUDA(cudaMemcpyAsync(&Cn, P<int64_t>(W.conn_off) + n, 8, cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
+    MV_RB(&Cn, P<int64_t>(W.conn_off) + n, 8);
     if (ensure(ctx, W.conn, 4 * (size_t)std::max<int64_t>(Cn, 1))) return MV_ERR_OOM;
     launch_csr_fill(fin, F, P<int64_t>(W.face_off), P<int64_t>(W.conn_off), P<int32_t>(W.in_count),
                     P<int32_t>(W.cursor), ni, P<int32_t>(W.conn), st);
@@ -1250,8 +1281,7 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
     launch_batch_csr(fin, F, P<int64_t>(W.face_off), P<int32_t>(W.face_count), ni, d_pos, nj,
                      P<int32_t>(W.in_count), P<int32_t>(W.conn_count), st);
     scan_i32_to_i64(P<int32_t>(W.conn_count), ntot, P<int64_t>(W.conn_off), P<long long>(W.scan_tmp), st);
-    MV_CUDA(cudaMemcpyAsync(&Cn, P<int64_t>(W.conn_off) + ntot, 8, cudaMemcpyDeviceToHost, st));
-    MV_CUDA(cudaStreamSynchronize(st));
+    MV_RB(&Cn, P<int64_t>(W.conn_off) + ntot, 8);
     if (ensure(ctx, W.conn, 4 * (size_t)std::max<int64_t>(Cn, 1))) return MV_ERR_OOM;
     launch_batch_csr_fill(fin, F, P<int64_t>(W.face_off), P<int64_t>(W.conn_off), P<int32_t>(W.in_count),
                           P<int32_t>(W.cursor), ni, d_pos, nj, P<int32_t>(W.conn), st);
@@ -1265,11 +1295,8 @@ int build_batch_device_impl(mv_context* ctx, const double* d_xyz, const uint8_t*
   ctx->bj_cell.assign(pos.begin(), pos.end());
   ctx->bj_face.assign(nj + 1, 0);
   ctx->bj_conn.assign(nj + 1, 0);
-  MV_CUDA(cudaMemcpyAsync(ctx->bj_face.data(), W.b_fbase.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost,
-                          st));
-  if (owned)
-    MV_CUDA(cudaMemcpyAsync(ctx->bj_conn.data(), W.b_cbconn.p, 8 * (size_t)(nj + 1), cudaMemcpyDeviceToHost,
-                            st));
+  MV_RB(ctx->bj_face.data(), W.b_fbase.p, 8 * (size_t)(nj + 1));
+  if (owned) MV_RB(ctx->bj_conn.data(), W.b_cbconn.p, 8 * (size_t)(nj + 1));
   MV_CUDA(cudaGetLastError());
   MV_CUDA(cudaStreamSynchronize(st));
   stats.device_bytes = (int64_t)ctx->dev_bytes;
@@ -1697,6 +1724,16 @@ int mv_context_create(int device, mv_context** out) {
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, dev);
   for (int i = 0; i < 10 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+  // the readback buffer; without it readbacks fall back to cudaMemcpy
+  if (e == cudaSuccess) {
+    if (cudaHostAlloc(&ctx->rb_host, READBACK_BYTES, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&ctx->rb_dev, ctx->rb_host, 0) != cudaSuccess) {
+      cudaGetLastError();
+      if (ctx->rb_host) cudaFreeHost(ctx->rb_host);
+      ctx->rb_host = nullptr;
+      ctx->rb_dev = nullptr;
+    }
+  }
   if (e != cudaSuccess) {
     delete ctx;
     return cuda_status(e);
@@ -1725,6 +1762,7 @@ void mv_context_destroy(mv_context* ctx) {
     if (bufs[i].p) cudaFree(bufs[i].p);
   if (ctx->host) cudaFreeHost(ctx->host);
   if (ctx->host_cells) cudaFreeHost(ctx->host_cells);
+  if (ctx->rb_host) cudaFreeHost(ctx->rb_host);
   for (cudaEvent_t ev : ctx->stage_ev) cudaEventDestroy(ev);
   for (int i = 0; i < 10; i++)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
