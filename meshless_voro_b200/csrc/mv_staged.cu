@@ -55,29 +55,95 @@ __device__ __forceinline__ int stage_pos(const StageJob& SJ, int item) {
 }
 
 // ------------------------------------------------------------------- shell --
+// Bitonic sort of 32 * EPL entries in registers (element i = lane + 32 e in slot e of
+// every lane) by the squared distance alone, carrying the list word; as sort_regs.
+template <int EPL>
+__device__ __forceinline__ void sort_regs_key(unsigned long long (&key)[EPL], uint32_t (&val)[EPL],
+                                              int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * EPL; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int e = 0; e < EPL; e++) {
+          const int pe = e ^ (j >> 5);
+          if (pe > e) {
+            const bool asc = ((32 * e) & k) == 0;
+            if ((key[e] > key[pe]) == asc) {
+              const unsigned long long tk = key[e];
+              const uint32_t tv = val[e];
+              key[e] = key[pe], val[e] = val[pe];
+              key[pe] = tk, val[pe] = tv;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < EPL; e++) {
+          const unsigned long long ok = __shfl_xor_sync(FULL, key[e], j);
+          const uint32_t ov = __shfl_xor_sync(FULL, val[e], j);
+          const bool asc = (((lane + 32 * e) & k) == 0);
+          const bool lower = (lane & j) == 0;
+          if ((key[e] > ok) == (lower == asc)) key[e] = ok, val[e] = ov;
+        }
+      }
+    }
+  }
+}
+
 // Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
 // sorted position * 27 + shift code; returns whether the nearest entry is the
-// generator itself.
+// generator itself (sorted position spos, no shift).  The entries are sorted by their
+// squared distance alone; only when two of them share one (lattice-like inputs) is the
+// shell sorted again by (squared distance, original index, shift code), the stream's
+// full order.
 template <int EPL>
 __device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, int lane, int cnt,
-                                               int self, uint32_t* out) {
+                                               int self, int spos, uint32_t* out) {
   unsigned long long key[EPL];
-  uint32_t tie[EPL];
-  int32_t pos[EPL];
+  uint32_t val[EPL];
 #pragma unroll
   for (int e = 0; e < EPL; e++) {
     const int i = lane + 32 * e;
     key[e] = i < cnt ? B.key[i] : ~0ull;
-    tie[e] = i < cnt ? B.tie[i] : ~0u;
-    pos[e] = i < cnt ? B.cpos[i] : 0;
+    val[e] = i < cnt ? (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u : 0u;
   }
-  sort_regs<EPL>(key, tie, pos, lane);
+  sort_regs_key<EPL>(key, val, lane);
+  // equal squared distances end next to each other: element i against i + 1
+  bool dup = false;
+#pragma unroll
+  for (int e = 0; e < EPL; e++) {
+    const unsigned long long nx = __shfl_down_sync(FULL, key[e], 1);
+    const unsigned long long wrap = __shfl_sync(FULL, key[e + 1 < EPL ? e + 1 : e], 0);
+    const unsigned long long next = lane < 31 ? nx : wrap;
+    const int i = lane + 32 * e;
+    dup |= (i + 1 < cnt) && (lane < 31 || e + 1 < EPL) && key[e] == next;
+  }
+  if (__any_sync(FULL, dup)) {
+    uint32_t tie[EPL];
+    int32_t pos[EPL];
+#pragma unroll
+    for (int e = 0; e < EPL; e++) {
+      const int i = lane + 32 * e;
+      key[e] = i < cnt ? B.key[i] : ~0ull;
+      tie[e] = i < cnt ? B.tie[i] : ~0u;
+      pos[e] = i < cnt ? B.cpos[i] : 0;
+    }
+    sort_regs<EPL>(key, tie, pos, lane);
+#pragma unroll
+    for (int e = 0; e < EPL; e++) {
+      const int i = lane + 32 * e;
+      if (i < cnt) out[i] = (uint32_t)pos[e] * 27u + tie[e] % 27u;
+    }
+    return (int)(__shfl_sync(FULL, tie[0], 0) / 27u) == self;
+  }
 #pragma unroll
   for (int e = 0; e < EPL; e++) {
     const int i = lane + 32 * e;
-    if (i < cnt) out[i] = (uint32_t)pos[e] * 27u + tie[e] % 27u;
+    if (i < cnt) out[i] = val[e];
   }
-  return (int)(__shfl_sync(FULL, tie[0], 0) / 27u) == self;
+  return __shfl_sync(FULL, val[0], 0) == (uint32_t)spos * 27u + 13u;
 }
 
 template <int WARPS, bool MULTI>
@@ -131,11 +197,11 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB)
     uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
     bool self_first;
     if (cnt <= 32)
-      self_first = sort_and_write<1>(B, lane, cnt, self, out);
+      self_first = sort_and_write<1>(B, lane, cnt, self, spos, out);
     else if (cnt <= 64)
-      self_first = sort_and_write<2>(B, lane, cnt, self, out);
+      self_first = sort_and_write<2>(B, lane, cnt, self, spos, out);
     else
-      self_first = sort_and_write<4>(B, lane, cnt, self, out);
+      self_first = sort_and_write<4>(B, lane, cnt, self, spos, out);
     // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
     // fused kernel reports the error otherwise
     if (lane == 0) {
