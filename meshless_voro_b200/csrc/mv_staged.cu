@@ -428,7 +428,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
         const bool two = nv > 32 && lane + 32 < nv;
         if (two) fv2 = S.f4[S.ord[lane + 32]];
         for (;;) {
-          const unsigned run = k < 32 ? ~(mfilt >> k) : 0u;  // a set bit ends the run
+          const unsigned run = ~(mfilt >> k);  // k < 32: a set bit ends the run
           const int c = k < limit ? min(run ? __ffs(run) - 1 : 32, min(4, limit - k)) : 0;  // filterable in a row
           if (c <= 0) break;
           unsigned needm = 0u;
