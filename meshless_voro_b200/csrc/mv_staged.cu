@@ -421,33 +421,19 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const int limit = evt ? __ffs(evt) - 1 : wn;
       const int k0 = k;
       if (PREC == MV_PRECISION_FILTERED) {
-        // candidates certified to remove no vertex are consumed without their plane,
-        // up to four per round: their tests are independent, so the rounds' votes
-        // overlap instead of waiting on one another
-        float4 fv2 = make_float4(0.f, 0.f, 0.f, 0.f);  // this lane's second vertex
-        const bool two = nv > 32 && lane + 32 < nv;
-        if (two) fv2 = S.f4[S.ord[lane + 32]];
-        for (;;) {
-          const unsigned run = ~(mfilt >> k);  // k < 32: a set bit ends the run
-          const int c = k < limit ? min(run ? __ffs(run) - 1 : 32, min(4, limit - k)) : 0;  // filterable in a row
-          if (c <= 0) break;
-          unsigned needm = 0u;
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            if (j < c) {
-              const float4 fk = S.wf[k + j];
-              const float2 ck = S.wc[k + j];
-              const float Tk = __fmaf_ru(ck.y, A32, ck.x);
-              bool need = lane < nv && !(fmaf(fk.z, fv.z, fmaf(fk.y, fv.y, fmaf(fk.x, fv.x, fk.w))) > Tk);
-              if (two) need = need || !(fmaf(fk.z, fv2.z, fmaf(fk.y, fv2.y, fmaf(fk.x, fv2.x, fk.w))) > Tk);
-              needm |= (unsigned)__any_sync(FULL, need) << j;
-            }
+        // candidates certified to remove no vertex are consumed without their plane
+        while (k < limit && ((mfilt >> k) & 1u)) {
+          const float4 fk = S.wf[k];
+          const float2 ck = S.wc[k];
+          const float exk = fk.x, eyk = fk.y, ezk = fk.z, hk = fk.w;
+          const float Tk = __fmaf_ru(ck.y, A32, ck.x);
+          bool need = lane < nv && !(fmaf(ezk, fv.z, fmaf(eyk, fv.y, fmaf(exk, fv.x, hk))) > Tk);
+          if (nv > 32 && lane + 32 < nv) {
+            const float4 f = S.f4[S.ord[lane + 32]];
+            need = need || !(fmaf(ezk, f.z, fmaf(eyk, f.y, fmaf(exk, f.x, hk))) > Tk);
           }
-          if (needm) {
-            k += __ffs(needm) - 1;
-            break;
-          }
-          k += c;
+          if (__any_sync(FULL, need)) break;
+          k++;
         }
       }
       cc.neighbours(k - k0);
