@@ -645,6 +645,15 @@ __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, i
     }
   };
 
+  // the x-distances of the cells lo[0] .. hi[0] are the same for every row: with at
+  // most 32 of them, lane j holds cell lo[0] + j's and the rows read them by shuffle
+  const int nx = hi[0] - lo[0] + 1;
+  const bool xlanes = nx <= 32;
+  double dx2l = 0.0;
+  if (xlanes && lane < nx) {
+    const double dx = box_d(0, lo[0] + lane);
+    dx2l = dx * dx;
+  }
   for (int row0 = 0; row0 < nrows && count <= stop; row0 += 32) {
     const int row = row0 + lane;
     int nseg = 0;
@@ -653,19 +662,36 @@ __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, i
     // cell ranges holding a dense cell, deferred (one per image): c0 | c1 << 16, 0: none
     int dfr[3] = {-1, -1, -1};
     int my = 0, mz = 0, cy = 0, cz = 0;
+    int uy = 0, uz = 0;
+    double byz2 = 0.0;
+    bool rowin = false;
     if (row < nrows) {
-      const int uy = lo[1] + row % ny, uz = lo[2] + row / ny;
+      uy = lo[1] + row % ny, uz = lo[2] + row / ny;
       const double dy = box_d(1, uy), dz = box_d(2, uz);
-      const double byz2 = dy * dy + dz * dz;
-      if (all || byz2 < R2v) {
-        int first = 1 << 30, last = -(1 << 30);
-        for (int ux = lo[0]; ux <= hi[0]; ux++) {
-          double dx = box_d(0, ux);
-          if (all || dx * dx + byz2 < R2v) {
-            first = min(first, ux);
-            last = max(last, ux);
-          }
+      byz2 = dy * dy + dz * dz;
+      rowin = all || byz2 < R2v;
+    }
+    // the row's cells within the ball: the first and last x cell that pass
+    int first = 1 << 30, last = -(1 << 30);
+    if (xlanes) {
+      for (int j = 0; j < nx; j++) {
+        const double dx2 = __shfl_sync(FULL, dx2l, j);
+        if (rowin && (all || dx2 + byz2 < R2v)) {
+          first = min(first, lo[0] + j);
+          last = max(last, lo[0] + j);
         }
+      }
+    } else if (rowin) {
+      for (int ux = lo[0]; ux <= hi[0]; ux++) {
+        double dx = box_d(0, ux);
+        if (all || dx * dx + byz2 < R2v) {
+          first = min(first, ux);
+          last = max(last, ux);
+        }
+      }
+    }
+    if (row < nrows) {
+      if (rowin) {
         const int Gx = J.G[0], Gy = J.G[1], Gz = J.G[2];
         my = uy < 0 ? -1 : (uy >= Gy ? 1 : 0);
         mz = uz < 0 ? -1 : (uz >= Gz ? 1 : 0);
