@@ -1020,6 +1020,92 @@ __device__ __noinline__ int ring_replay_warp(SM& S, int lane, int nvf, int nv, i
   return len;
 }
 
+// ring_replay_warp for at most 32 removed vertices with each triangle held by its lane:
+// lane j starts with the triangle at position nvf + j and tracks the position the
+// reference's swaps give it (the triangle at position i moves to the winner's position
+// when step i takes a later one), so a step is a reduction of the positions of the
+// triangles that extend the cycle rather than a scan of shared memory.  The removed
+// vertices' order in `ord` is left as it was: only their slots are reused, and the
+// vertices that replace them take ring order.  Returns as ring_replay_warp.
+template <class T, class SM>
+__device__ __noinline__ int ring_replay_lanes(SM& S, int lane, int nvf, int nv, int np) {
+  using PIdx = typename T::PIdx;
+  const int n = nv - nvf;
+  if (n > 32) return ring_replay_warp<T>(S, lane, nvf, nv, np);
+  for (int i = lane; i < np; i += 32) S.rptr[i] = (PIdx)i;
+  int t[3] = {0, 0, 0};
+  if (lane < n) {
+    const int sl = S.ord[nvf + lane];
+    t[0] = S.vd0[sl], t[1] = S.vd1[sl], t[2] = S.vd2[sl];
+  }
+  int pos = lane;
+  bool open = lane > 0 && lane < n;  // not yet part of the cycle
+  int start = __shfl_sync(FULL, t[0], 0);
+  __syncwarp();
+  if (lane == 0) {
+    S.rptr[t[0]] = (PIdx)t[1];
+    S.rptr[t[1]] = (PIdx)t[2];
+    S.rptr[t[2]] = (PIdx)t[0];
+  }
+  __syncwarp();
+  int len = 3;
+  for (int i = 1; i < n; i++) {
+    int code = 0;  // 1 + 2 * rotation + case (0: grow the cycle, 1: absorb a node)
+    if (open) {
+      const bool in[3] = {S.rptr[t[0]] != (PIdx)t[0], S.rptr[t[1]] != (PIdx)t[1],
+                          S.rptr[t[2]] != (PIdx)t[2]};
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        const int j = a == 2 ? 0 : a + 1, k = a == 0 ? 2 : a - 1;
+        if (code == 0) {
+          if (!in[a] && in[j] && in[k] && S.rptr[t[k]] == (PIdx)t[j])
+            code = 1 + 2 * a;
+          else if (in[a] && in[j] && in[k] && S.rptr[t[k]] == (PIdx)t[j] && S.rptr[t[j]] == (PIdx)t[a])
+            code = 2 + 2 * a;
+        }
+      }
+    }
+    const unsigned key = code ? (unsigned)pos : 64u;
+    const unsigned m = __reduce_min_sync(FULL, key);
+    if (m == 64u) return -1;
+    const int w = __ffs(__ballot_sync(FULL, key == m)) - 1;
+    const int how = __shfl_sync(FULL, code, w);
+    const int a = (how - 1) >> 1;
+    const int w0 = __shfl_sync(FULL, t[0], w), w1 = __shfl_sync(FULL, t[1], w),
+              w2 = __shfl_sync(FULL, t[2], w);
+    const int ta = a == 0 ? w0 : (a == 1 ? w1 : w2);
+    const int tb = a == 0 ? w1 : (a == 1 ? w2 : w0);
+    const int tc = a == 0 ? w2 : (a == 1 ? w0 : w1);
+    const bool grow = ((how - 1) & 1) == 0;
+    __syncwarp();
+    if (lane == 0) {
+      S.rptr[tc] = (PIdx)ta;
+      S.rptr[grow ? ta : tb] = (PIdx)tb;
+    }
+    if (lane == w) open = false;
+    else if (open && pos == i) pos = (int)m;  // swap(i, m) of compute_boundary
+    if (grow) {
+      len += 1;
+    } else {
+      if (start == tb) start = ta;
+      len -= 1;
+    }
+    __syncwarp();
+  }
+  if (len > T::VMAX) return -2;
+  if (lane == 0) {
+    int cur = start;
+    for (int e = 0; e < len; e++) {
+      const int nxt = S.rptr[cur];
+      S.ea[e] = (PIdx)cur;
+      S.eb[e] = (PIdx)nxt;
+      cur = nxt;
+    }
+  }
+  __syncwarp();
+  return len;
+}
+
 // Parallel ring: the boundary edges of the union of the removed dual triangles form
 // the same cycle the serial algorithm builds; it starts at the first removed
 // vertex's dual[0] whenever that node is still on the boundary.  Returns the edge

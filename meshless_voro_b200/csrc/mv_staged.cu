@@ -568,7 +568,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       int E = ring_ranked<T>(S, lane, nvf, nv, &eu, &ew, &erank);
       if (E < 0) {
         cc.serial_ring();
-        E = ring_replay_warp<T>(S, lane, nvf, nv, np);
+        E = ring_replay_lanes<T>(S, lane, nvf, nv, np);
         if (E == -2) return CELL_OVERFLOW;
         if (E < 0) {
           *err_code = MV_ERR_RING;
