@@ -860,81 +860,12 @@ __device__ __forceinline__ void sort_regs(unsigned long long (&key)[EPL], uint32
 }
 
 // -------------------------------------------------------------------- ring --
-// Serial replay of compute_boundary (convex_cell.rs:421-441) and SimpleCycle
-// (simple_cycle.rs:17-78) on lane 0 for the removed vertices at positions [nvf, nv).
-// Produces the edge list (S.ea, S.eb) and returns its length, -1 on failure, -2 when
-// the ring exceeds the tier's vertex capacity.
-template <class T, class SM>
-__device__ __noinline__ int ring_serial(SM& S, int nvf, int nv, int np) {
-  using PIdx = typename T::PIdx;
-  for (int i = 0; i < np; i++) S.rptr[i] = (PIdx)i;
-  auto contains = [&](int i) { return S.rptr[i] != (PIdx)i; };
-  const int s0 = S.ord[nvf];
-  int start = S.vd0[s0];
-  int len = 3;
-  {
-    int a = S.vd0[s0], b = S.vd1[s0], c = S.vd2[s0];
-    S.rptr[a] = (PIdx)b;
-    S.rptr[b] = (PIdx)c;
-    S.rptr[c] = (PIdx)a;
-  }
-  const int n = nv - nvf;
-  for (int i = 1; i < n; i++) {
-    int idx = i;
-    for (;;) {
-      if (idx >= n) return -1;
-      const int sl = S.ord[nvf + idx];
-      const int t0 = S.vd0[sl], t1 = S.vd1[sl], t2 = S.vd2[sl];
-      const bool i0 = contains(t0), i1 = contains(t1), i2 = contains(t2);
-      bool ok = false;
-      for (int a = 0; a < 3 && !ok; a++) {
-        // rotation (ta, tb, tc) = (tri[a], tri[a+1], tri[a+2])
-        const int ta = a == 0 ? t0 : (a == 1 ? t1 : t2);
-        const int tb = a == 0 ? t1 : (a == 1 ? t2 : t0);
-        const int tc = a == 0 ? t2 : (a == 1 ? t0 : t1);
-        const bool ia = a == 0 ? i0 : (a == 1 ? i1 : i2);
-        const bool ib = a == 0 ? i1 : (a == 1 ? i2 : i0);
-        const bool ic = a == 0 ? i2 : (a == 1 ? i0 : i1);
-        if (!ia && ib && ic && S.rptr[tc] == (PIdx)tb) {
-          S.rptr[tc] = (PIdx)ta;
-          S.rptr[ta] = (PIdx)tb;
-          len += 1;
-          ok = true;
-        } else if (ia && ib && ic && S.rptr[tc] == (PIdx)tb && S.rptr[tb] == (PIdx)ta) {
-          S.rptr[tc] = (PIdx)ta;
-          S.rptr[tb] = (PIdx)tb;
-          if (start == tb) start = ta;
-          len -= 1;
-          ok = true;
-        }
-      }
-      if (ok) {
-        if (idx > i) {
-          const PIdx tmp = S.ord[nvf + i];
-          S.ord[nvf + i] = S.ord[nvf + idx];
-          S.ord[nvf + idx] = tmp;
-        }
-        break;
-      }
-      idx++;
-    }
-  }
-  if (len > T::VMAX) return -2;
-  int cur = start;
-  for (int e = 0; e < len; e++) {
-    const int nxt = S.rptr[cur];
-    S.ea[e] = (PIdx)cur;
-    S.eb[e] = (PIdx)nxt;
-    cur = nxt;
-  }
-  return len;
-}
-
-// The same replay of compute_boundary + SimpleCycle with the whole warp: step i of the
-// reference's loop takes the first removed vertex at or after position i whose dual
-// triangle extends the cycle (failed try_extend calls change nothing), so one ballot
-// over the candidates, 32 at a time, finds it; the rotation / case order of try_extend
-// is kept per candidate.  The cycle's successor pointers end in S.rptr and its
+// Replay of compute_boundary (convex_cell.rs:421-441) + SimpleCycle
+// (simple_cycle.rs:17-78) for the removed vertices at positions [nvf, nv), with the
+// whole warp: step i of the reference's loop takes the first removed vertex at or after
+// position i whose dual triangle extends the cycle (failed try_extend calls change
+// nothing), so one ballot over the candidates, 32 at a time, finds it; the rotation /
+// case order of try_extend is kept per candidate.  The cycle's successor pointers end in S.rptr and its
 // iteration order in (S.ea, S.eb); returns the edge count, -1 on failure, -2 when the
 // ring exceeds the tier's vertex capacity.
 template <class T, class SM>
