@@ -401,6 +401,11 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
   SJ.rec_off = P<int64_t>(W.rec_off);
   SJ.rec = P<double>(W.rec);
   SJ.rec_cap = rec_cap;
+  SJ.full_records = keep_records ? 1 : 0;
+  // box-corner band tests (quantised lattices) are decided by the clip kernel's box
+  // form, in the probe chunk and, when the probe met them in every cell on average,
+  // in every later chunk
+  bool box_mode = false;
   SJ.retry_list = P<int32_t>(W.retry);
   SJ.retry_count = reinterpret_cast<unsigned int*>(ctr);
   // cells that need the exact predicate skip the wide round: they join the list the
@@ -412,6 +417,7 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
     SJ.nitems = (int32_t)chunks[c].second;
     SJ.work = reinterpret_cast<unsigned int*>(ctr + 1 + 3 * c);
     SJ.rec_counter = keep_records ? keep_records : ctr + 1 + 3 * c + 2;
+    SJ.box = ((probe && c == 0) || box_mode) ? 1 : 0;
     const int64_t warps_needed = SJ.nitems;
     for (int k = 0; k < 3; k++) {
       const int wpb = 4;  // every stage kernel runs 4 warps per block
@@ -423,10 +429,12 @@ int run_staged(mv_context* ctx, const Job& J, const JobTable& TB, int dim, const
     }
     MV_CUDA(cudaEventRecord(ctx->stage_ev[4 * c + 3], st));
     if (probe && c == 0) {
-      unsigned long long pc[2] = {0, 0};
+      unsigned long long pc[3] = {0, 0, 0};
       MV_RB(&pc[0], ctr, 8);
       MV_RB(&pc[1], ctr + ctr2, 8);
+      MV_RB(&pc[2], J.stats + ST_EXACT, 8);
       const int64_t n_exact = (int64_t)(pc[1] & 0xffffffffull);
+      box_mode = (int64_t)pc[2] >= (int64_t)SJ.nitems;
       if (2 * n_exact >= SJ.nitems) {
         // the fused kernel's list: the probe's exact cells, its retries, then every
         // cell after the probe

@@ -158,6 +158,20 @@ __device__ __noinline__ int exact_clip(const Job& J, const SM& S, int s, D3 x, D
   return in_sphere_exact_sign(A, B, C, Dd, W);
 }
 
+// Whether the exact decision of exact_clip is the zero determinant of five corners of
+// one axis-aligned box (box_corners), found without multi-limb arithmetic: the vertex
+// is then kept.
+template <class SM>
+__device__ __noinline__ bool exact_clip_box_zero(const Job& J, const SM& S, int s, D3 x, D3 ngb) {
+  int64_t A[3], B[3], C[3], Dd[3], W[3];
+  iloc(J, x, A);
+  iloc(J, right_loc(J, S, S.vd0[s], x), B);
+  iloc(J, right_loc(J, S, S.vd1[s], x), C);
+  iloc(J, right_loc(J, S, S.vd2[s], x), Dd);
+  iloc(J, ngb, W);
+  return box_corners(A, B, C, Dd, W);
+}
+
 // Vertex::from_dual (convex_cell.rs:28-48) into slot `slot`; *r2 receives the
 // vertex's squared distance to the generator (kept in S.vr2 when STORE_R2; otherwise
 // vertex_r2 recomputes it).
@@ -1181,23 +1195,46 @@ __device__ __forceinline__ int ring_ranked(SM& S, int lane, int nvf, int nv, int
 
 // ------------------------------------------------------------ cell records --
 // A finished cell as the staged integral kernel and the cell export read it, in words:
-// header (np, nv as int32), safety radius, plane normals / offsets / generator
-// projections (7 np f64), vertex locations in the reference's order (3 nv f64), right
-// generators (int32), plane shift codes and vertex duals (bytes).
-__host__ __device__ __forceinline__ int64_t rec_words(int np, int nv) {
-  return 2 + 7 * (int64_t)np + 3 * (int64_t)nv + (np + 1) / 2 + (np + 3 * nv + 7) / 8;
+// header (np as int32; nv | flags as int32), safety radius, then for the stored planes
+// pl in [pb, np): normals / offsets / generator projections (7 (np - pb) f64); the
+// vertex locations in the reference's order (3 nv f64); the stored planes' right
+// generators (int32); their shift codes and the vertex duals (bytes, the duals as
+// plane indices).
+//
+// A compact record (the plain builds) leaves out the six boundary planes when no
+// vertex lies on one of them (pb = 6): the integral step reads a plane only through a
+// vertex dual.  A full record (export builds: the cell export reads every plane) keeps
+// them (pb = 0).  Recomputing the vertex locations from their dual planes instead of
+// storing them was measured slower (the integral kernel's three IEEE divisions per
+// vertex cost more than the loads they save).
+constexpr int REC_PB6 = 1 << 16;  // nv word flag: planes start at 6
+
+__host__ __device__ __forceinline__ int64_t rec_words(int np, int nv, int pb = 0) {
+  const int ps = np - pb;
+  return 2 + 7 * (int64_t)ps + 3 * (int64_t)nv + (ps + 1) / 2 + (ps + 3 * nv + 7) / 8;
 }
 
 // Writes the cell held in shared memory (SM layout, see the top of this file, plus
-// bisector_point(J, k, x), the HalfSpace point p of plane k) as a record at words
-// allocated from *counter in rec[0, cap), and its offset to *off_slot.  Returns false
-// when the buffer is full or a plane index does not fit the record's bytes.
+// bisector_point(J, k, x), the HalfSpace point p of plane k) as a record (full or
+// compact) at words allocated from *counter in rec[0, cap), and its offset to
+// *off_slot.  Returns false when the buffer is full or a plane index does not fit the
+// record's bytes.
 template <class SM>
 __device__ bool write_record(const Job& J, double* rec, int64_t cap, unsigned long long* counter,
                              int64_t* off_slot, const SM& S, int lane, D3 x, int np, int nv,
-                             double sr) {
+                             double sr, bool full) {
   if (np > 255) return false;
-  const int64_t words = rec_words(np, nv);
+  int pb = 0;
+  if (!full) {
+    bool onb = false;
+    for (int q = lane; q < nv; q += 32) {
+      const int sl = S.ord[q];
+      onb |= S.vd0[sl] < 6 || S.vd1[sl] < 6 || S.vd2[sl] < 6;
+    }
+    pb = __any_sync(FULL, onb) ? 0 : 6;
+  }
+  const int ps = np - pb;
+  const int64_t words = rec_words(np, nv, pb);
   unsigned long long off = 0;
   if (lane == 0) off = atomicAdd(counter, (unsigned long long)words);
   off = __shfl_sync(FULL, off, 0);
@@ -1205,22 +1242,23 @@ __device__ bool write_record(const Job& J, double* rec, int64_t cap, unsigned lo
   double* R = rec + off;
   if (lane == 0) {
     reinterpret_cast<int32_t*>(R)[0] = np;
-    reinterpret_cast<int32_t*>(R)[1] = nv;
+    reinterpret_cast<int32_t*>(R)[1] = nv | (pb ? REC_PB6 : 0);
     R[1] = sr;
   }
   double* nx = R + 2;
-  double *ny = nx + np, *nz = ny + np, *dd = nz + np, *qx = dd + np, *qy = qx + np, *qz = qy + np;
-  double *vxo = qz + np, *vyo = vxo + nv, *vzo = vyo + nv;
+  double *ny = nx + ps, *nz = ny + ps, *dd = nz + ps, *qx = dd + ps, *qy = qx + ps, *qz = qy + ps;
+  double *vxo = qz + ps, *vyo = vxo + nv, *vzo = vyo + nv;
   int32_t* rt = reinterpret_cast<int32_t*>(vzo + nv);
-  uint8_t* pc = reinterpret_cast<uint8_t*>(vzo + nv + (np + 1) / 2);
-  uint8_t *d0 = pc + np, *d1 = d0 + nv, *d2 = d1 + nv;
-  for (int pl = lane; pl < np; pl += 32) {
+  uint8_t* pc = reinterpret_cast<uint8_t*>(vzo + nv + (ps + 1) / 2);
+  uint8_t *d0 = pc + ps, *d1 = d0 + nv, *d2 = d1 + nv;
+  for (int k = lane; k < ps; k += 32) {
+    const int pl = k + pb;
     const D3 nn = {S.pnx[pl], S.pny[pl], S.pnz[pl]};
     const D3 pr = plane_project(nn, S.bisector_point(J, pl, x), x);  // Plane::project_onto
-    nx[pl] = nn.x, ny[pl] = nn.y, nz[pl] = nn.z, dd[pl] = S.pd[pl];
-    qx[pl] = pr.x, qy[pl] = pr.y, qz[pl] = pr.z;
-    rt[pl] = S.pright[pl];
-    pc[pl] = S.pcode[pl];
+    nx[k] = nn.x, ny[k] = nn.y, nz[k] = nn.z, dd[k] = S.pd[pl];
+    qx[k] = pr.x, qy[k] = pr.y, qz[k] = pr.z;
+    rt[k] = S.pright[pl];
+    pc[k] = S.pcode[pl];
   }
   for (int q = lane; q < nv; q += 32) {
     const int sl = S.ord[q];
@@ -1232,29 +1270,40 @@ __device__ bool write_record(const Job& J, double* rec, int64_t cap, unsigned lo
   return true;
 }
 
-// The record at R as the integral step reads it (see integrate_view).
+// The record at R as the integral step and the cell export read it.  Plane accessors
+// take the plane index pl (>= pb).
 struct RecordView {
   const double *nx, *ny, *nz, *dd, *qx, *qy, *qz, *vx, *vy, *vz;
   const int32_t* rt;
   const uint8_t *pc, *d0, *d1, *d2;
-  int np, nv;
+  int np, nv, pb;
   double sr;
   __device__ explicit RecordView(const double* R) {
     np = __ldg(reinterpret_cast<const int32_t*>(R));
-    nv = __ldg(reinterpret_cast<const int32_t*>(R) + 1);
+    const int w = __ldg(reinterpret_cast<const int32_t*>(R) + 1);
+    nv = w & 0xffff;
+    pb = (w & REC_PB6) ? 6 : 0;
     sr = __ldg(R + 1);
-    nx = R + 2, ny = nx + np, nz = ny + np, dd = nz + np;
-    qx = dd + np, qy = qx + np, qz = qy + np;
-    vx = qz + np, vy = vx + nv, vz = vy + nv;
+    const int ps = np - pb;
+    // plane arrays indexed by pl - pb
+    nx = R + 2, ny = nx + ps, nz = ny + ps, dd = nz + ps;
+    qx = dd + ps, qy = qx + ps, qz = qy + ps;
+    vx = qz + ps, vy = vx + nv, vz = vy + nv;
     rt = reinterpret_cast<const int32_t*>(vz + nv);
-    pc = reinterpret_cast<const uint8_t*>(vz + nv + (np + 1) / 2);
-    d0 = pc + np, d1 = d0 + nv, d2 = d1 + nv;
+    pc = reinterpret_cast<const uint8_t*>(vz + nv + (ps + 1) / 2);
+    d0 = pc + ps, d1 = d0 + nv, d2 = d1 + nv;
   }
-  __device__ D3 normal(int pl) const { return {__ldg(nx + pl), __ldg(ny + pl), __ldg(nz + pl)}; }
-  __device__ double d(int pl) const { return __ldg(dd + pl); }
-  __device__ D3 proj(int pl) const { return {__ldg(qx + pl), __ldg(qy + pl), __ldg(qz + pl)}; }
-  __device__ int right(int pl) const { return __ldg(rt + pl); }
-  __device__ int code(int pl) const { return __ldg(pc + pl); }
+  __device__ D3 normal(int pl) const {
+    const int k = pl - pb;
+    return {__ldg(nx + k), __ldg(ny + k), __ldg(nz + k)};
+  }
+  __device__ double d(int pl) const { return __ldg(dd + pl - pb); }
+  __device__ D3 proj(int pl) const {
+    const int k = pl - pb;
+    return {__ldg(qx + k), __ldg(qy + k), __ldg(qz + k)};
+  }
+  __device__ int right(int pl) const { return __ldg(rt + pl - pb); }
+  __device__ int code(int pl) const { return __ldg(pc + pl - pb); }
   __device__ int dual(int q, int i) const {
     return i == 0 ? __ldg(d0 + q) : (i == 1 ? __ldg(d1 + q) : __ldg(d2 + q));
   }
@@ -1277,11 +1326,14 @@ __device__ __forceinline__ bool line_projection(const View& V, int q, int i, D3 
 // Scratch of the integral step: projections on the plane-pair lines of STEP vertices
 // and their 6 STEP tets' values (rows padded so that lanes reading different rows at
 // the same column hit different banks).
-template <int STEP = 5>
+// With PM > 0, pm[pl] collects per step the (vertex, dual slot) pairs of plane pl as
+// bits 3 vl + i (zero between steps), so that a face sums only its own tets.
+template <int STEP = 5, int PM = 0>
 struct TetScratch {
   static constexpr int NT = 6 * STEP;
   double ix[3 * STEP], iy[3 * STEP], iz[3 * STEP];
   double val[8][NT + 3];
+  uint32_t pm[PM > 0 ? PM : 1];
 };
 
 // Integrals and face emission of a finished cell (convex_cell.rs:131-187,
@@ -1291,8 +1343,8 @@ struct TetScratch {
 // step of STEP vertices (STEP <= 10) projects on their 3 STEP plane-pair lines (one
 // per lane), builds their 6 STEP tets and accumulates them in the reference's tet
 // order: lanes 0-3 the cell integrals, lane p (and p + 32k) the integrals of face p.
-template <class T, int STEP, class View>
-__device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetScratch<STEP>& Sc,
+template <class T, int STEP, int PM, class View>
+__device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetScratch<STEP, PM>& Sc,
                                               int lane, int self, D3 x, int nv, int np, double sr,
                                               int* err_code) {
   static_assert(3 * STEP <= 32, "one projection per lane");
@@ -1318,6 +1370,14 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
     if (__any_sync(FULL, !ok)) {
       *err_code = MV_ERR_DET;
       return CELL_ERROR;
+    }
+    if constexpr (PM >= T::PMAX) {
+      if (lane < nstep) {
+        const int q = base + lane;
+        atomicOr(&Sc.pm[V.dual(q, 0)], 1u << (3 * lane));
+        atomicOr(&Sc.pm[V.dual(q, 1)], 1u << (3 * lane + 1));
+        atomicOr(&Sc.pm[V.dual(q, 2)], 1u << (3 * lane + 2));
+      }
     }
     __syncwarp();
     // DecompositionWithoutFaces: tet t of a vertex = (proj[t], proj[(t+5)%6], vertex)
@@ -1350,24 +1410,52 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
     if (lane < 4) {
       for (int s = 0; s < ntet; s++) cacc = cacc + Sc.val[lane][s];
     }
+    if constexpr (PM >= T::PMAX) {
+      // face pl: its vertices of this step in vertex order (ascending bits)
 #pragma unroll
-    for (int k = 0; k < T::PMAX / 32; k++) {
-      const int pl = lane + 32 * k;
-      if (pl < np) {
-        for (int vl = 0; vl < nstep; vl++) {
-          const int q = base + vl;
-          const int kk = V.dual(q, 0) == pl ? 0 : (V.dual(q, 1) == pl ? 1 : (V.dual(q, 2) == pl ? 2 : -1));
-          if (kk >= 0) {
-            const int s = 6 * vl + 2 * kk;
-            fa[k] = fa[k] + Sc.val[4][s];
-            fcx[k] = fcx[k] + Sc.val[5][s];
-            fcy[k] = fcy[k] + Sc.val[6][s];
-            fcz[k] = fcz[k] + Sc.val[7][s];
-            fa[k] = fa[k] + Sc.val[4][s + 1];
-            fcx[k] = fcx[k] + Sc.val[5][s + 1];
-            fcy[k] = fcy[k] + Sc.val[6][s + 1];
-            fcz[k] = fcz[k] + Sc.val[7][s + 1];
-            ftouched |= 1u << k;
+      for (int k = 0; k < T::PMAX / 32; k++) {
+        const int pl = lane + 32 * k;
+        unsigned m = 0u;
+        if (pl < np) {
+          m = Sc.pm[pl];
+          if (m) Sc.pm[pl] = 0u;
+        }
+        if (m) ftouched |= 1u << k;
+        while (m) {
+          const int b = __ffs(m) - 1;
+          m &= m - 1u;
+          const int vl = (b * 11) >> 5;  // b / 3 for b < 32
+          const int s = 6 * vl + 2 * (b - 3 * vl);
+          fa[k] = fa[k] + Sc.val[4][s];
+          fcx[k] = fcx[k] + Sc.val[5][s];
+          fcy[k] = fcy[k] + Sc.val[6][s];
+          fcz[k] = fcz[k] + Sc.val[7][s];
+          fa[k] = fa[k] + Sc.val[4][s + 1];
+          fcx[k] = fcx[k] + Sc.val[5][s + 1];
+          fcy[k] = fcy[k] + Sc.val[6][s + 1];
+          fcz[k] = fcz[k] + Sc.val[7][s + 1];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < T::PMAX / 32; k++) {
+        const int pl = lane + 32 * k;
+        if (pl < np) {
+          for (int vl = 0; vl < nstep; vl++) {
+            const int q = base + vl;
+            const int kk = V.dual(q, 0) == pl ? 0 : (V.dual(q, 1) == pl ? 1 : (V.dual(q, 2) == pl ? 2 : -1));
+            if (kk >= 0) {
+              const int s = 6 * vl + 2 * kk;
+              fa[k] = fa[k] + Sc.val[4][s];
+              fcx[k] = fcx[k] + Sc.val[5][s];
+              fcy[k] = fcy[k] + Sc.val[6][s];
+              fcz[k] = fcz[k] + Sc.val[7][s];
+              fa[k] = fa[k] + Sc.val[4][s + 1];
+              fcx[k] = fcx[k] + Sc.val[5][s + 1];
+              fcy[k] = fcy[k] + Sc.val[6][s + 1];
+              fcz[k] = fcz[k] + Sc.val[7][s + 1];
+              ftouched |= 1u << k;
+            }
           }
         }
       }

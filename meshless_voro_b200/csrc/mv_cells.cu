@@ -462,7 +462,7 @@ __device__ int build_cell(const Job& J, CellSmem<T>& S, int lane, int spos, cons
   }
   const int res = integrate_cell(J, S, lane, self, x, nv, np, sr, err_code);
   if (res == CELL_DONE && J.rec != nullptr &&
-      !write_record(J, J.rec, J.rec_cap, J.rec_counter, J.rec_off + spos, S, lane, x, np, nv, sr))
+      !write_record(J, J.rec, J.rec_cap, J.rec_counter, J.rec_off + spos, S, lane, x, np, nv, sr, true))
     return CELL_REC_OVERFLOW;
   return res;
 }

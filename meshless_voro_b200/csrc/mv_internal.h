@@ -154,6 +154,8 @@ struct StageJob {
   double* rec;                // cell records (planes, vertices) for the integral kernel
   int64_t rec_cap;            // record words available to the chunk
   unsigned long long* rec_counter;
+  int32_t full_records;       // 1: full records (export builds), 0: compact (write_record)
+  int32_t box;                // 1: the clip kernel decides box-corner band tests itself
   unsigned int* work;         // [3] work counters of the shell, clip and integral kernels
   int32_t* retry_list;        // positions the next round (wide round, fused kernel) takes
   unsigned int* retry_count;

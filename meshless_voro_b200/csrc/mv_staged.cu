@@ -302,6 +302,9 @@ struct ClipSmem {
   float2 wc[32];  // bound coefficients (c0, c1)
   uint32_t wpk[32];  // original index * 27 + shift code
   __device__ D3 plane_point(const Job& J, int k) const { return {J.bp[k][0], J.bp[k][1], J.bp[k][2]}; }
+  // coordinate c (0: x, 1: y, 2: z) arrays of the plane normals and vertex locations
+  __device__ const double* pn(int c) const { return c == 0 ? pnx : (c == 1 ? pny : pnz); }
+  __device__ double* vc(int c) { return c == 0 ? vx : (c == 1 ? vy : vz); }
   // HalfSpace::p of plane k: the boundary point, or (x + ngb) / 2 recomputed as at the clip
   __device__ D3 bisector_point(const Job& J, int k, D3 x) const {
     const int rr = pright[k];
@@ -313,19 +316,89 @@ struct ClipSmem {
   }
 };
 
-// Event counts of one clipped cell in two warp-uniform registers: a = neighbours
-// (16 bits) | planes (8) | serial rings (8), b = f32-undecided tests.  A cell of the
-// clip tier consumes at most 1023 neighbours and holds at most 64 planes and 64
-// vertices, so no field overflows (the clip kernel runs no exact test).
+// Event counts of one clipped cell in warp-uniform registers: a = neighbours (16
+// bits) | planes (8) | serial rings (8), b = f32-undecided tests, e = exact tests (all
+// of them box-corner zeros).  A cell of the clip tier consumes at most 1023 neighbours
+// and holds at most 64 planes and 64 vertices, so no field of a overflows.
 struct ClipCount {
-  unsigned a, b;
+  unsigned a, b, e;
   __device__ void neighbours(unsigned v) { a += v; }
   __device__ void plane() { a += 1u << 16; }
   __device__ void serial_ring() { a += 1u << 24; }
   __device__ void undecided(unsigned v) { b += v; }
+  __device__ void exact(unsigned v) { e += v; }
 };
 
-template <class T, int PREC>
+// Vertex::from_dual (convex_cell.rs:38-42) for the ring's E new vertices, three lanes
+// per vertex: lane 3e + c computes coordinate c of intersect_planes (geometry.rs:68-76)
+// of the planes (u, w, p_idx) of edge e, with the operations the whole-vector form
+// performs for that coordinate (((d0 (n1 x n2)_c + d1 (n2 x n0)_c) + d2 (n0 x n1)_c) /
+// det, det = n2 . (n0 x n1) on each of the three lanes), so every coordinate is the
+// same binary64 number.  Lane e < E holds edge e in (eu, ew, erank) when `ranked`,
+// otherwise the edges are S.ea / S.eb in ring order.  Stores the vertices at slots
+// ord[nvf + rank] and raises *mk to their squared radii (on lanes 3e).  Returns false
+// when a determinant is zero.
+template <class T>
+__device__ __forceinline__ bool new_vertices(ClipSmem<T>& S, int lane, int E, bool ranked, int eu,
+                                             int ew, int erank, int nvf, int p_idx, D3 x, int dim,
+                                             double* mk) {
+  using PIdx = typename T::PIdx;
+  const int el = (lane * 11) >> 5;  // lane / 3 for lane < 32
+  const int c = lane - 3 * el;
+  const int c1 = c == 2 ? 0 : c + 1, c2 = c == 0 ? 2 : c - 1;
+  const double* P1 = S.pn(c1);
+  const double* P2 = S.pn(c2);
+  const double xc = c == 0 ? x.x : (c == 1 ? x.y : x.z);
+  bool ok = true;
+  for (int e0 = 0; e0 < E; e0 += 10) {
+    const int e = e0 + el;
+    const bool act = lane < 30 && e < E;
+    int u, w, pos;
+    if (ranked) {
+      u = __shfl_sync(FULL, eu, e & 31);
+      w = __shfl_sync(FULL, ew, e & 31);
+      pos = __shfl_sync(FULL, erank, e & 31);
+    } else {
+      u = act ? (int)S.ea[e] : 0;
+      w = act ? (int)S.eb[e] : 0;
+      pos = e;
+    }
+    double coord = 0.0;
+    int slot = 0;
+    if (act) {
+      slot = S.ord[nvf + pos];
+      const int i = u, j = w, k = p_idx;
+      const D3 n0 = {S.pnx[i], S.pny[i], S.pnz[i]};
+      const D3 n1 = {S.pnx[j], S.pny[j], S.pnz[j]};
+      const D3 n2 = {S.pnx[k], S.pny[k], S.pnz[k]};
+      const double det = det_cols(n0, n1, n2);
+      if (det == 0.0) {
+        ok = false;
+      } else {
+        const double a1 = P1[i], a2 = P2[i], b1 = P1[j], b2 = P2[j], g1 = P1[k], g2 = P2[k];
+        const double y12 = b1 * g2 - g1 * b2;  // (n1 x n2)_c
+        const double y20 = g1 * a2 - a1 * g2;  // (n2 x n0)_c
+        const double y01 = a1 * b2 - b1 * a2;  // (n0 x n1)_c
+        coord = ((S.pd[i] * y12 + S.pd[j] * y20) + S.pd[k] * y01) / det;
+        S.vc(c)[slot] = coord;
+        reinterpret_cast<float*>(&S.f4[slot])[c] = __double2float_rn(coord - xc);
+        (c == 0 ? S.vd0 : (c == 1 ? S.vd1 : S.vd2))[slot] = (PIdx)(c == 0 ? i : (c == 1 ? j : k));
+      }
+    }
+    // squared radius (Vertex::from_dual) on lane 3e from the coordinates of lanes 3e + 1, 3e + 2
+    const double cy = __shfl_down_sync(FULL, coord, 1), cz = __shfl_down_sync(FULL, coord, 2);
+    if (act && c == 0) {
+      const D3 dl = {coord, dim >= 2 ? cy : 0.0, dim == 3 ? cz : 0.0};
+      const D3 r = sub(x, dl);
+      *mk = fmax(*mk, dot(r, r));
+    }
+  }
+  return __all_sync(FULL, ok);
+}
+
+// BOX: band tests that are box-corner zeros are decided here (the kernel used for
+// lattice-like inputs; the check's registers slow the common kernel by about a tenth).
+template <class T, int PREC, bool BOX>
 __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int lane, int item,
                          int self, int info, int* err_code, ClipCount& cc) {
   using PIdx = typename T::PIdx;
@@ -463,11 +536,12 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const double d = S.wd[e];
       unsigned rm[T::NW];
       int n_und = 0;
-      bool need_exact = false;
+      int bsl[T::NW];  // slot of this lane's vertex when its f64 test is in the band
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
         const int q = lane + 32 * w;
         bool removed = false;
+        bsl[w] = -1;
         if (q < nv) {
           const int sl = S.ord[q];
           bool decided = false;
@@ -482,16 +556,37 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           if (!decided) {
             n_und++;
             const double c = dot(n, D3{S.vx[sl], S.vy[sl], S.vz[sl]}) - d;
-            need_exact |= fabs(c) < errb;
-            removed = c < 0.0;
+            if (fabs(c) < errb)
+              bsl[w] = sl;
+            else
+              removed = c < 0.0;
           }
         }
         rm[w] = __ballot_sync(FULL, removed);
       }
       // inside the f64 band the reference decides with the exact in-sphere predicate
-      // (half_space.rs:40-47); its multi-limb arithmetic does not fit this kernel's
-      // register budget, so the fused kernel builds such cells (before any change here)
-      if (__any_sync(FULL, need_exact)) return CELL_EXACT;
+      // (half_space.rs:40-47), a zero determinant keeping the vertex.  Five corners of
+      // one axis-aligned box (every band test of a quantised lattice) are such a zero
+      // without multi-limb arithmetic (BOX); any other band test sends the cell, before
+      // any change here, to the fused kernel (the multi-limb predicate does not fit
+      // this kernel's register budget)
+      if (__any_sync(FULL, bsl[0] >= 0 || (T::NW > 1 && bsl[T::NW - 1] >= 0))) {
+        if constexpr (BOX) {
+          const uint32_t pk = S.wpk[e];
+          const int cand = (int)(pk / 27u), code = (int)(pk % 27u);
+          D3 ngb = load_gen(J, cand);
+          if (code != 13) ngb = add(ngb, D3{J.shift[code][0], J.shift[code][1], J.shift[code][2]});
+          bool hard = false;
+          unsigned nb = 0;
+#pragma unroll
+          for (int w = 0; w < T::NW; w++)
+            if (bsl[w] >= 0) hard |= !exact_clip_box_zero(J, S, bsl[w], x, ngb), nb++;
+          if (__any_sync(FULL, hard)) return CELL_EXACT;
+          cc.exact(__reduce_add_sync(FULL, nb));
+        } else {
+          return CELL_EXACT;
+        }
+      }
       n_und = (int)__reduce_add_sync(FULL, (unsigned)n_und);
       if (PREC == MV_PRECISION_FILTERED) cc.undecided(n_und);
       int nrem = 0;
@@ -513,14 +608,42 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       cc.plane();
 
       // swap-remove loop (convex_cell.rs:365-390) as a closed-form permutation of ord
-      // over 64-bit masks of removed / kept positions; kept vertices before nvf stay.
-      // The s-th removed / kept position comes from inverse maps built in S.ea / S.eb
-      // (free until the ring below).
+      // over masks of removed / kept positions; kept vertices before nvf stay.  The
+      // s-th removed / kept position comes from inverse maps built in S.ea / S.eb (free
+      // until the ring below).  Cells of at most 32 vertices (most clips) take 32-bit
+      // masks, one position per lane.
       const unsigned long long rm64 = ((unsigned long long)rm[1] << 32) | rm[0];
       const unsigned long long km64 = ~rm64 & (nv >= 64 ? ~0ull : ((1ull << nv) - 1ull));
       const int totK = __popcll(km64);
       const int nvf = totK;
-      {
+      if (nv <= 32) {
+        const unsigned rm32 = rm[0], km32 = (unsigned)km64;
+        const unsigned below = lanemask_lt();
+        const bool in = lane < nv, gone = (rm32 >> lane) & 1u;
+        const int rr = __popc(rm32 & below), rk = __popc(km32 & below);
+        if (in) {
+          if (gone)
+            S.ea[rr] = (PIdx)lane;
+          else
+            S.eb[rk] = (PIdx)lane;
+        }
+        __syncwarp();
+        int dd = -1;
+        PIdx held = 0;
+        if (in) {
+          if (!gone) {
+            if (lane >= nvf) dd = S.ea[totK - rk - 1];
+          } else if (lane <= nvf) {
+            dd = ((rr == 0) ? nv : (int)S.eb[totK - rr]) - 1;
+          } else {
+            dd = lane - 1;
+          }
+          if (dd >= 0) held = S.ord[lane];
+        }
+        __syncwarp();
+        if (dd >= 0) S.ord[dd] = held;
+        __syncwarp();
+      } else {
 #pragma unroll
         for (int w = 0; w < 2; w++) {
           const int q = lane + 32 * w;
@@ -566,6 +689,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       // gets the boundary edge at ring position erank and creates its vertex
       int eu = 0, ew = 0, erank = 0;
       int E = ring_ranked<T>(S, lane, nvf, nv, &eu, &ew, &erank);
+      const bool replayed = E < 0;
       if (E < 0) {
         cc.serial_ring();
         E = ring_replay_lanes<T>(S, lane, nvf, nv, np);
@@ -574,21 +698,9 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
           *err_code = MV_ERR_RING;
           return CELL_ERROR;
         }
-        if (lane < E) eu = S.ea[lane], ew = S.eb[lane];
-        erank = lane;
       }
       if (nvf + E > T::VMAX) return CELL_OVERFLOW;
-      bool ok = true;
-      double r2n = 0.0;
-      if (lane < E) {
-        ok = make_vertex<PIdx, false>(S, S.ord[nvf + erank], eu, ew, p_idx, x, dim, &r2n);
-        mk = fmax(mk, r2n);
-      }
-      for (int ei = lane + 32; ei < E; ei += 32) {  // rings of more than 32 edges (serial replay)
-        ok &= make_vertex<PIdx, false>(S, S.ord[nvf + ei], S.ea[ei], S.eb[ei], p_idx, x, dim, &r2n);
-        mk = fmax(mk, r2n);
-      }
-      if (__any_sync(FULL, !ok)) {
+      if (!new_vertices<T>(S, lane, E, !replayed, eu, ew, erank, nvf, p_idx, x, dim, &mk)) {
         *err_code = MV_ERR_DET;
         return CELL_ERROR;
       }
@@ -612,12 +724,13 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
   if (!finished && !(exhausted || sr < SJ.rad[item] * (1.0 - 1e-12))) return CELL_RETRY;
 
   // ---- the cell record for the integral kernel ----
-  if (!write_record(J, SJ.rec, SJ.rec_cap, SJ.rec_counter, SJ.rec_off + item, S, lane, x, np, nv, sr))
+  if (!write_record(J, SJ.rec, SJ.rec_cap, SJ.rec_counter, SJ.rec_off + item, S, lane, x, np, nv, sr,
+                    SJ.full_records != 0))
     return CELL_RETRY;
   return CELL_DONE;
 }
 
-template <class T, int PREC, int WARPS, bool MULTI>
+template <class T, int PREC, int WARPS, bool MULTI, bool BOX>
 __global__ void __launch_bounds__(32 * WARPS, T::MINB)
     clip_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
                 const __grid_constant__ JobTable TB) {
@@ -653,15 +766,15 @@ __global__ void __launch_bounds__(32 * WARPS, T::MINB)
     const int info = SJ.info[item];
     int res = CELL_RETRY;
     int err = 0;
-    ClipCount cc{0u, 0u};
-    if (info > 0) res = clip_cell<T, PREC>(J, SJ, S, lane, item, self, info, &err, cc);
+    ClipCount cc{0u, 0u, 0u};
+    if (info > 0) res = clip_cell<T, PREC, BOX>(J, SJ, S, lane, item, self, info, &err, cc);
     __syncwarp();
     if (lane == 0) {
       if (res == CELL_DONE) {
-        const unsigned v[4] = {cc.a & 0xffffu, (cc.a >> 16) & 0xffu, cc.a >> 24, cc.b};
-        const int slot[4] = {ST_NEIGHBOURS, ST_PLANES, ST_SERIAL_RING, ST_F32_UNDECIDED};
+        const unsigned v[5] = {cc.a & 0xffffu, (cc.a >> 16) & 0xffu, cc.a >> 24, cc.b, cc.e};
+        const int slot[5] = {ST_NEIGHBOURS, ST_PLANES, ST_SERIAL_RING, ST_F32_UNDECIDED, ST_EXACT};
 #pragma unroll
-        for (int i = 0; i < 4; i++)
+        for (int i = 0; i < 5; i++)
           if (v[i]) atomicAdd(&cnt[slot[i]], (unsigned long long)v[i]);
       } else {
         SJ.rec_off[item] = -1;
@@ -689,8 +802,10 @@ template <class T, int WARPS, bool MULTI>
 __global__ void __launch_bounds__(32 * WARPS, MV_INT_MINB)
     integrate_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
                      const __grid_constant__ JobTable TB) {
-  __shared__ TetScratch<INT_STEP> scratch[WARPS];
+  __shared__ TetScratch<INT_STEP, T::PMAX> scratch[WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = lane; i < T::PMAX; i += 32) scratch[warp].pm[i] = 0u;
+  __syncwarp();
   unsigned done = 0;
   for (;;) {
     int item = 0;
@@ -741,9 +856,9 @@ int stage_blocks_per_sm(int kernel, int precision) {
   if (kernel == 3) return occupancy(shell_wide_kernel<WIDE_WARPS, false>, 32 * WIDE_WARPS, WIDE_SMEM);
   if (kernel == 1)
     return precision == MV_PRECISION_FILTERED
-               ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, false>,
+               ? occupancy(clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, false, false>,
                            32 * CLIP_WARPS, CLIP_SMEM)
-               : occupancy(clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, false>,
+               : occupancy(clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, false, false>,
                            32 * CLIP_WARPS, CLIP_SMEM);
   return occupancy(integrate_kernel<TierClip, INT_WARPS, false>, 32 * INT_WARPS, 0);
 }
@@ -777,8 +892,14 @@ static cudaError_t launch_stage_t(int kernel, const Job& J, const StageJob& SJ, 
     k<<<blocks, 32 * WIDE_WARPS, WIDE_SMEM, st>>>(J, SJ, TB);
   } else if (kernel == 1) {
     auto k = J.precision == MV_PRECISION_FILTERED
-                 ? clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, MULTI>
-                 : clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, MULTI>;
+                 ? clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, MULTI, false>
+                 : clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, MULTI, false>;
+    if constexpr (!MULTI) {
+      if (SJ.box)
+        k = J.precision == MV_PRECISION_FILTERED
+                ? clip_kernel<TierClip, MV_PRECISION_FILTERED, CLIP_WARPS, false, true>
+                : clip_kernel<TierClip, MV_PRECISION_FP64, CLIP_WARPS, false, true>;
+    }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CLIP_SMEM);
     if (e != cudaSuccess) return e;
     k<<<blocks, 32 * CLIP_WARPS, CLIP_SMEM, st>>>(J, SJ, TB);

@@ -57,8 +57,9 @@ def test_c2_exact_lattice_64_full(gpu_ctx, oracle, precision, pipeline):
     assert st["exact_tests"] > 0
     assert st["cells_built"] == 64 ** 3
     if pipeline == "auto":
-        # the probe chunk finds an exact-heavy input: the fused kernel builds the rest
-        assert st["ms_shell"] > 0 and st["staged_retries"] >= 0.9 * 64 ** 3
+        # every band test of the lattice is a box-corner zero, which the staged clip
+        # kernel decides itself: the staged pipeline builds the lattice
+        assert st["ms_shell"] > 0 and st["staged_retries"] < 0.1 * 64 ** 3
 
 
 _SAMPLES = {}
