@@ -47,7 +47,7 @@ HBM_PEAK_FALLBACK = 6650.0
 # DRAM bytes (read + write) per cell of the clip kernel, from one ncu capture of the
 # clip kernel on the 64^3 periodic Poisson case; traffic grows in proportion to the
 # cells, so a launch's traffic is this figure times its cells.
-CLIP_KERNEL_DRAM_BYTES_PER_CELL = 2420.0
+CLIP_KERNEL_DRAM_BYTES_PER_CELL = 2026.0
 # algorithmic bytes (generator read + cell outputs + owned faces + CSR entries)
 BYTES_GEN, BYTES_CELL, BYTES_FACE, BYTES_CONN = 24, 40, 68, 4
 # cells per chunk of the staged pipeline (library default)
