@@ -1324,15 +1324,16 @@ __device__ __forceinline__ bool line_projection(const View& V, int q, int i, D3 
 
 // --------------------------------------------------------------- integrals --
 // Scratch of the integral step: projections on the plane-pair lines of STEP vertices
-// and their 6 STEP tets' values (rows padded so that lanes reading different rows at
-// the same column hit different banks).
+// and their 6 STEP tets' values (rows 16-byte aligned, read two tets at a time, and
+// padded by 6 values so that lanes reading different rows at the same column hit
+// different banks).
 // With PM > 0, pm[pl] collects per step the (vertex, dual slot) pairs of plane pl as
 // bits 3 vl + i (zero between steps), so that a face sums only its own tets.
 template <int STEP = 5, int PM = 0>
 struct TetScratch {
   static constexpr int NT = 6 * STEP;
   double ix[3 * STEP], iy[3 * STEP], iz[3 * STEP];
-  double val[8][NT + 3];
+  alignas(16) double val[8][NT + 6];
   uint32_t pm[PM > 0 ? PM : 1];
 };
 
@@ -1408,7 +1409,11 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
     __syncwarp();
     const int ntet = 6 * nstep;
     if (lane < 4) {
-      for (int s = 0; s < ntet; s++) cacc = cacc + Sc.val[lane][s];
+      for (int s = 0; s < ntet; s += 2) {  // ntet is even
+        const double2 v = *reinterpret_cast<const double2*>(&Sc.val[lane][s]);
+        cacc = cacc + v.x;
+        cacc = cacc + v.y;
+      }
     }
     if constexpr (PM >= T::PMAX) {
       // face pl: its vertices of this step in vertex order (ascending bits)
@@ -1426,14 +1431,18 @@ __device__ __forceinline__ int integrate_view(const Job& J, const View& V, TetSc
           m &= m - 1u;
           const int vl = (b * 11) >> 5;  // b / 3 for b < 32
           const int s = 6 * vl + 2 * (b - 3 * vl);
-          fa[k] = fa[k] + Sc.val[4][s];
-          fcx[k] = fcx[k] + Sc.val[5][s];
-          fcy[k] = fcy[k] + Sc.val[6][s];
-          fcz[k] = fcz[k] + Sc.val[7][s];
-          fa[k] = fa[k] + Sc.val[4][s + 1];
-          fcx[k] = fcx[k] + Sc.val[5][s + 1];
-          fcy[k] = fcy[k] + Sc.val[6][s + 1];
-          fcz[k] = fcz[k] + Sc.val[7][s + 1];
+          const double2 a2 = *reinterpret_cast<const double2*>(&Sc.val[4][s]);
+          const double2 x2 = *reinterpret_cast<const double2*>(&Sc.val[5][s]);
+          const double2 y2 = *reinterpret_cast<const double2*>(&Sc.val[6][s]);
+          const double2 z2 = *reinterpret_cast<const double2*>(&Sc.val[7][s]);
+          fa[k] = fa[k] + a2.x;
+          fcx[k] = fcx[k] + x2.x;
+          fcy[k] = fcy[k] + y2.x;
+          fcz[k] = fcz[k] + z2.x;
+          fa[k] = fa[k] + a2.y;
+          fcx[k] = fcx[k] + x2.y;
+          fcy[k] = fcy[k] + y2.y;
+          fcz[k] = fcz[k] + z2.y;
         }
       }
     } else {

@@ -45,7 +45,7 @@ constexpr int INT_WARPS = 4;
 #endif
 constexpr int INT_STEP = MV_INT_STEP;  // vertices per step of the integral kernel
 #ifndef MV_INT_MINB
-#define MV_INT_MINB 8
+#define MV_INT_MINB 7
 #endif
 using TierClip = Tier<64, 64, SHELL_CMAX, 8, uint8_t, MV_CLIP_MINB>;
 
@@ -283,12 +283,14 @@ struct ClipSmem {
   using PIdx = typename T::PIdx;
   // clipping planes (half_space.rs:9-19); planes 0-5 are the boundary, the others
   // bisectors whose point p = (x + ngb) / 2 is recomputed from the right generator
-  double pnx[T::PMAX], pny[T::PMAX], pnz[T::PMAX], pd[T::PMAX];
+  // (one f64 of padding after each coordinate array: the three lanes of a new vertex
+  // read and write the same index of all three arrays, now in different banks)
+  double pnx[T::PMAX], pad_nx, pny[T::PMAX], pad_ny, pnz[T::PMAX], pd[T::PMAX];
   int32_t pright[T::PMAX];  // original index of the right generator, -1: boundary
   uint8_t pcode[T::PMAX];   // periodic shift code, 13: none
   PIdx rptr[T::PMAX];       // ring successor (SimpleCycle::ptrs)
   // vertices (convex_cell.rs:16-25) in fixed slots
-  double vx[T::VMAX], vy[T::VMAX], vz[T::VMAX];
+  double vx[T::VMAX], pad_vx, vy[T::VMAX], pad_vy, vz[T::VMAX];
   float4 f4[T::VMAX];  // f32 (v - x) for the filter
   uint32_t plm[T::PMAX];  // ring_ranked: lanes whose removed triangle holds the plane
   alignas(4) PIdx ord[T::VMAX];   // position -> slot; [0, nv) is the reference's order
