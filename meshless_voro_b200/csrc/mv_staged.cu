@@ -56,10 +56,9 @@ __device__ __forceinline__ int stage_pos(const StageJob& SJ, int item) {
 
 // ------------------------------------------------------------------- shell --
 // Bitonic sort of 32 * EPL entries in registers (element i = lane + 32 e in slot e of
-// every lane) by the squared distance alone, carrying the list word; as sort_regs.
+// every lane) by a 32-bit key alone, carrying the list word; as sort_regs.
 template <int EPL>
-__device__ __forceinline__ void sort_regs_key(unsigned long long (&key)[EPL], uint32_t (&val)[EPL],
-                                              int lane) {
+__device__ __forceinline__ void sort_regs_key(uint32_t (&key)[EPL], uint32_t (&val)[EPL], int lane) {
 #pragma unroll
   for (int k = 2; k <= 32 * EPL; k <<= 1) {
 #pragma unroll
@@ -71,7 +70,7 @@ __device__ __forceinline__ void sort_regs_key(unsigned long long (&key)[EPL], ui
           if (pe > e) {
             const bool asc = ((32 * e) & k) == 0;
             if ((key[e] > key[pe]) == asc) {
-              const unsigned long long tk = key[e];
+              const uint32_t tk = key[e];
               const uint32_t tv = val[e];
               key[e] = key[pe], val[e] = val[pe];
               key[pe] = tk, val[pe] = tv;
@@ -81,7 +80,7 @@ __device__ __forceinline__ void sort_regs_key(unsigned long long (&key)[EPL], ui
       } else {
 #pragma unroll
         for (int e = 0; e < EPL; e++) {
-          const unsigned long long ok = __shfl_xor_sync(FULL, key[e], j);
+          const uint32_t ok = __shfl_xor_sync(FULL, key[e], j);
           const uint32_t ov = __shfl_xor_sync(FULL, val[e], j);
           const bool asc = (((lane + 32 * e) & k) == 0);
           const bool lower = (lane & j) == 0;
@@ -95,42 +94,46 @@ __device__ __forceinline__ void sort_regs_key(unsigned long long (&key)[EPL], ui
 // Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
 // sorted position * 27 + shift code; returns whether the nearest entry is the
 // generator itself (sorted position spos, no shift).  The entries are sorted by their
-// squared distance alone; only when two of them share one (lattice-like inputs) is the
-// shell sorted again by (squared distance, original index, shift code), the stream's
-// full order.
+// squared distance rounded down to f32 (a monotone map, so distinct keys order the
+// entries as their squared distances do); only when two keys are equal (distances
+// within an f32 ulp, or equal as in lattice-like inputs) is the shell sorted again by
+// (squared distance, original index, shift code), the stream's full order.
 template <int EPL>
 __device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, int lane, int cnt,
                                                int self, int spos, uint32_t* out) {
-  unsigned long long key[EPL];
+  uint32_t key[EPL];
   uint32_t val[EPL];
 #pragma unroll
   for (int e = 0; e < EPL; e++) {
     const int i = lane + 32 * e;
-    key[e] = i < cnt ? B.key[i] : ~0ull;
+    // d2 >= 0 is finite: its f32 bit pattern orders as the value, below the padding
+    key[e] = i < cnt ? __float_as_uint(__double2float_rd(__longlong_as_double((long long)B.key[i])))
+                     : ~0u;
     val[e] = i < cnt ? (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u : 0u;
   }
   sort_regs_key<EPL>(key, val, lane);
-  // equal squared distances end next to each other: element i against i + 1
+  // equal keys end next to each other: element i against i + 1
   bool dup = false;
 #pragma unroll
   for (int e = 0; e < EPL; e++) {
-    const unsigned long long nx = __shfl_down_sync(FULL, key[e], 1);
-    const unsigned long long wrap = __shfl_sync(FULL, key[e + 1 < EPL ? e + 1 : e], 0);
-    const unsigned long long next = lane < 31 ? nx : wrap;
+    const uint32_t nx = __shfl_down_sync(FULL, key[e], 1);
+    const uint32_t wrap = __shfl_sync(FULL, key[e + 1 < EPL ? e + 1 : e], 0);
+    const uint32_t next = lane < 31 ? nx : wrap;
     const int i = lane + 32 * e;
     dup |= (i + 1 < cnt) && (lane < 31 || e + 1 < EPL) && key[e] == next;
   }
   if (__any_sync(FULL, dup)) {
+    unsigned long long dkey[EPL];
     uint32_t tie[EPL];
     int32_t pos[EPL];
 #pragma unroll
     for (int e = 0; e < EPL; e++) {
       const int i = lane + 32 * e;
-      key[e] = i < cnt ? B.key[i] : ~0ull;
+      dkey[e] = i < cnt ? B.key[i] : ~0ull;
       tie[e] = i < cnt ? B.tie[i] : ~0u;
       pos[e] = i < cnt ? B.cpos[i] : 0;
     }
-    sort_regs<EPL>(key, tie, pos, lane);
+    sort_regs<EPL>(dkey, tie, pos, lane);
 #pragma unroll
     for (int e = 0; e < EPL; e++) {
       const int i = lane + 32 * e;
