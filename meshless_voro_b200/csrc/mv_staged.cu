@@ -223,6 +223,41 @@ constexpr int WIDE_MIN = 384;
 constexpr int WIDE_WARPS = 4;
 constexpr size_t WIDE_SMEM = sizeof(ShellBuf<WIDE_CMAX>) * WIDE_WARPS;
 
+// Sorts the wide shell [0, n) by the squared distance rounded down to f32 (as
+// sort_and_write) in place of B.key: each key becomes that 32-bit key above the
+// entry's index, so one 64-bit word is compared and moved per entry.  Returns false
+// when two keys are equal (the order then needs the full (key, tie) sort, over the
+// original keys, which this overwrote).
+template <int CMAX>
+__device__ __noinline__ bool sort_shell_key32(ShellBuf<CMAX>& B, int lane, int n) {
+  int np2 = 32;
+  while (np2 < n) np2 <<= 1;
+  for (int i = lane; i < np2; i += 32) {
+    unsigned long long w = ~0ull;
+    if (i < n) {
+      const float k = __double2float_rd(__longlong_as_double((long long)B.key[i]));
+      w = ((unsigned long long)__float_as_uint(k) << 32) | (unsigned)i;
+    }
+    B.key[i] = w;
+  }
+  __syncwarp();
+  for (int k = 2; k <= np2; k <<= 1) {
+    for (int jl = __ffs(k) - 2; jl >= 0; jl--) {
+      const int j = 1 << jl;
+      for (int i = lane; i < (np2 >> 1); i += 32) {
+        const int lo = ((i >> jl) << (jl + 1)) | (i & (j - 1));
+        const int hi = lo + j;
+        const unsigned long long ka = B.key[lo], kb = B.key[hi];
+        if ((ka > kb) == ((lo & k) == 0)) B.key[lo] = kb, B.key[hi] = ka;
+      }
+      __syncwarp();
+    }
+  }
+  bool dup = false;
+  for (int i = lane; i + 1 < n; i += 32) dup |= (B.key[i] >> 32) == (B.key[i + 1] >> 32);
+  return !__any_sync(FULL, dup);
+}
+
 template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(32 * WARPS, 3)
     shell_wide_kernel(const __grid_constant__ Job J0, const __grid_constant__ StageJob SJ,
@@ -268,11 +303,23 @@ __global__ void __launch_bounds__(32 * WARPS, 3)
       if (lane == 0) SJ.info[item] = -1;
       continue;
     }
-    sort_shell<WIDE_CMAX>(B, lane, cnt);
     uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
-    for (int i = lane; i < cnt; i += 32) out[i] = (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u;
+    uint32_t first;  // the nearest entry's tie (original index * 27 + shift code)
+    if (sort_shell_key32<WIDE_CMAX>(B, lane, cnt)) {
+      for (int i = lane; i < cnt; i += 32) {
+        const int e = (int)(uint32_t)B.key[i];
+        out[i] = (uint32_t)B.cpos[e] * 27u + B.tie[e] % 27u;
+      }
+      first = B.tie[(uint32_t)B.key[0]];
+    } else {
+      // equal keys: the same shell again (the gather is deterministic), fully sorted
+      cnt = gather_shell<WIDE_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 4 * WIDE_CMAX);
+      sort_shell<WIDE_CMAX>(B, lane, cnt);
+      for (int i = lane; i < cnt; i += 32) out[i] = (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u;
+      first = B.tie[0];
+    }
     if (lane == 0) {
-      const bool self_first = (int)(B.tie[0] / 27u) == self;
+      const bool self_first = (int)(first / 27u) == self;
       SJ.info[item] = self_first ? (cnt | (all ? (1 << 30) : 0)) : -1;
       SJ.rad[item] = R;
     }
