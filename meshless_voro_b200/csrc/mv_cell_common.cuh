@@ -479,7 +479,7 @@ __device__ __forceinline__ int job_of(const JobTable& T, int pos) {
 // segment that contains a dense cell (J.dprefix) is deferred: its cells are then
 // visited one by one, and a dense cell contributes the octree cells that the shell
 // reaches.  Without the ball test (all images enumerated) every cell counts whole.
-template <int CMAX, bool BIG, bool DENSE>
+template <int CMAX, bool BIG, bool DENSE, bool CODE_ONLY>
 __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
                                               double lo2, const double* ext, bool* exhausted,
                                               int stop, char* big) {
@@ -549,7 +549,7 @@ __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, i
         s = B.sstart[a] + (t - B.spref[a]);
         const int code = B.scode[a];
         const double px = __ldg(J.sx + s), py = __ldg(J.sy + s), pz = __ldg(J.sz + s);
-        const int orig = __ldg(J.sid + s);
+        const int orig = CODE_ONLY ? 0 : __ldg(J.sid + s);
         if (J.periodic) {
           const double ddx = (x.x + J.qshift[code][0]) - px;
           const double ddy = (x.y + J.qshift[code][1]) - py;
@@ -561,7 +561,7 @@ __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, i
         }
         keep = (d2 >= lo2) && (d2 < R2);
         beyond += (d2 >= R2);
-        tie = (uint32_t)orig * 27u + (uint32_t)code;
+        tie = CODE_ONLY ? (uint32_t)code : (uint32_t)orig * 27u + (uint32_t)code;
       }
       const unsigned bal = __ballot_sync(FULL, keep);
       const int pos = count + __popc(bal & lanemask_lt());
@@ -783,13 +783,15 @@ __device__ __noinline__ int gather_shell_impl(const Job& J, ShellBuf<CMAX>& B, i
 
 // gather_shell_impl without the dense-cell code when the build has no dense cell (the
 // uniform-density case keeps its registers), with it otherwise.
-template <int CMAX, bool BIG = false>
+// With CODE_ONLY, B.tie holds the shift code alone (no load of the original index per
+// element); the caller completes it where the full order is needed.
+template <int CMAX, bool BIG = false, bool CODE_ONLY = false>
 __device__ __forceinline__ int gather_shell(const Job& J, ShellBuf<CMAX>& B, int lane, D3 x, double R,
                                             double lo2, const double* ext, bool* exhausted, int stop,
                                             char* big = nullptr) {
   return J.dprefix != nullptr
-             ? gather_shell_impl<CMAX, BIG, true>(J, B, lane, x, R, lo2, ext, exhausted, stop, big)
-             : gather_shell_impl<CMAX, BIG, false>(J, B, lane, x, R, lo2, ext, exhausted, stop, big);
+             ? gather_shell_impl<CMAX, BIG, true, CODE_ONLY>(J, B, lane, x, R, lo2, ext, exhausted, stop, big)
+             : gather_shell_impl<CMAX, BIG, false, CODE_ONLY>(J, B, lane, x, R, lo2, ext, exhausted, stop, big);
 }
 
 // Bitonic sort of the shell [0, n) by (key, tie) ascending, carrying cpos; n <= CMAX.

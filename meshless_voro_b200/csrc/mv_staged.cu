@@ -91,16 +91,16 @@ __device__ __forceinline__ void sort_regs_key(uint32_t (&key)[EPL], uint32_t (&v
   }
 }
 
-// Sorts the gathered shell (cnt <= 32 EPL entries) in registers and writes it as
-// sorted position * 27 + shift code; returns whether the nearest entry is the
-// generator itself (sorted position spos, no shift).  The entries are sorted by their
+// Sorts the gathered shell (cnt <= 32 EPL entries; B.tie holds the shift codes) in
+// registers and writes it as sorted position * 27 + shift code; returns whether the
+// nearest entry is the generator itself (sorted position spos, no shift).  The entries are sorted by their
 // squared distance rounded down to f32 (a monotone map, so distinct keys order the
 // entries as their squared distances do); only when two keys are equal (distances
 // within an f32 ulp, or equal as in lattice-like inputs) is the shell sorted again by
 // (squared distance, original index, shift code), the stream's full order.
 template <int EPL>
-__device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, int lane, int cnt,
-                                               int self, int spos, uint32_t* out) {
+__device__ __forceinline__ bool sort_and_write(const Job& J, const ShellBuf<SHELL_CMAX>& B, int lane,
+                                               int cnt, int self, int spos, uint32_t* out) {
   uint32_t key[EPL];
   uint32_t val[EPL];
 #pragma unroll
@@ -109,7 +109,7 @@ __device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, in
     // d2 >= 0 is finite: its f32 bit pattern orders as the value, below the padding
     key[e] = i < cnt ? __float_as_uint(__double2float_rd(__longlong_as_double((long long)B.key[i])))
                      : ~0u;
-    val[e] = i < cnt ? (uint32_t)B.cpos[i] * 27u + B.tie[i] % 27u : 0u;
+    val[e] = i < cnt ? (uint32_t)B.cpos[i] * 27u + B.tie[i] : 0u;
   }
   sort_regs_key<EPL>(key, val, lane);
   // equal keys end next to each other: element i against i + 1
@@ -130,7 +130,7 @@ __device__ __forceinline__ bool sort_and_write(const ShellBuf<SHELL_CMAX>& B, in
     for (int e = 0; e < EPL; e++) {
       const int i = lane + 32 * e;
       dkey[e] = i < cnt ? B.key[i] : ~0ull;
-      tie[e] = i < cnt ? B.tie[i] : ~0u;
+      tie[e] = i < cnt ? (uint32_t)__ldg(J.sid + B.cpos[i]) * 27u + B.tie[i] : ~0u;
       pos[e] = i < cnt ? B.cpos[i] : 0;
     }
     sort_regs<EPL>(dkey, tie, pos, lane);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB)
     const D3 x = load_gen(J, self);
     bool all = false;
     double R = first_radius(J, x, lane);
-    int cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
+    int cnt = gather_shell<SHELL_CMAX, false, true>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
     // the density estimate behind R is rough where the density varies: a shell that
     // overflows the list is pulled in, one far below a uniform region's ~92 candidates
     // (too small to close most cells) is widened, a few times at most
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB)
       else
         break;
       R *= f;
-      cnt = gather_shell<SHELL_CMAX>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
+      cnt = gather_shell<SHELL_CMAX, false, true>(J, B, lane, x, R, 0.0, ext, &all, 32 * SHELL_CMAX);
     }
     if (cnt > SHELL_CMAX || cnt == 0) {
       if (lane == 0) SJ.info[item] = -1;
@@ -200,11 +200,11 @@ __global__ void __launch_bounds__(32 * WARPS, MV_SHELL_MINB)
     uint32_t* out = SJ.cand + (int64_t)item * SJ.cstride;
     bool self_first;
     if (cnt <= 32)
-      self_first = sort_and_write<1>(B, lane, cnt, self, spos, out);
+      self_first = sort_and_write<1>(J, B, lane, cnt, self, spos, out);
     else if (cnt <= 64)
-      self_first = sort_and_write<2>(B, lane, cnt, self, spos, out);
+      self_first = sort_and_write<2>(J, B, lane, cnt, self, spos, out);
     else
-      self_first = sort_and_write<4>(B, lane, cnt, self, spos, out);
+      self_first = sort_and_write<4>(J, B, lane, cnt, self, spos, out);
     // the first neighbour must be the generator itself (convex_cell.rs:325-329); the
     // fused kernel reports the error otherwise
     if (lane == 0) {
