@@ -4,14 +4,14 @@
 #pragma once
 // {dimensionality, pipeline, n_min, n_max, initial_radius, points_per_grid_cell, chunk_cells, reserved}
 static const mv_tuning_entry kBuiltinTuning[] = {
-    {3, MV_PIPELINE_STAGED, 0, 8192, 2.8, 4.0, 1048576, 0},
+    {3, MV_PIPELINE_STAGED, 0, 8192, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 8192, 32768, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 32768, 131072, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 131072, 524288, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 524288, 2097152, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 2097152, 8388608, 2.8, 2.2, 1048576, 0},
     {3, MV_PIPELINE_STAGED, 8388608, 4611686018427387904LL, 2.8, 2.2, 1048576, 0},
-    {2, MV_PIPELINE_STAGED, 0, 8192, 3.2, 2.2, 1048576, 0},
+    {2, MV_PIPELINE_STAGED, 0, 8192, 2.4, 2.2, 1048576, 0},
     {2, MV_PIPELINE_STAGED, 8192, 32768, 3.2, 2.2, 1048576, 0},
     {2, MV_PIPELINE_STAGED, 32768, 131072, 3.2, 2.2, 1048576, 0},
     {2, MV_PIPELINE_STAGED, 131072, 524288, 3.2, 2.2, 1048576, 0},
