@@ -588,7 +588,7 @@ __device__ int clip_cell(const Job& J, const StageJob& SJ, ClipSmem<T>& S, int l
       const double d = S.wd[e];
       unsigned rm[T::NW];
       int n_und = 0;
-      int bsl[T::NW];  // slot of this lane's vertex when its f64 test is in the band
+      int bsl[T::NW];  // slot of this lane's vertex when its f64 test is in the band, else -1
 #pragma unroll
       for (int w = 0; w < T::NW; w++) {
         const int q = lane + 32 * w;
