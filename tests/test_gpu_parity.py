@@ -203,3 +203,20 @@ def test_duplicate_generators_raise(gpu_ctx, pipeline):
 def test_empty_input(gpu_ctx):
     a = gpu_ctx.build_arrays(np.zeros((0, 3)), None, [0, 0, 0], [1, 1, 1], 3, False)
     assert a.n_cells == 0 and len(a.face_left) == 0
+
+
+def test_plate_lattice_wide_round_ties(gpu_ctx, oracle):
+    """An exact lattice of thin plates (16 x 16 x 256 in the periodic unit box, 65,536
+    cells): the probe chunk selects the clip kernel's box form (every band test is a
+    box-corner zero), no first shell closes a cell (they are 16 times wider than
+    thick), and every wide-round shell is full of equal squared distances, so the wide
+    round's equal-key fallback (the shell gathered again and fully sorted) builds them."""
+    i = (np.arange(16) + 0.5) / 16
+    k = (np.arange(256) + 0.5) / 256
+    g = np.stack(np.meshgrid(i, i, k, indexing="ij"), -1).reshape(-1, 3)
+    orc = oracle.build(g, [0, 0, 0], [1, 1, 1], dim=3, periodic=True)
+    for precision in ("filtered", "fp64"):
+        gpu = gpu_ctx.build_arrays(g, None, [0, 0, 0], [1, 1, 1], 3, True, precision=precision)
+        assert compare(gpu, orc), "expected bit-identical integrals"
+        st = gpu_ctx.last_stats()
+        assert st["staged_wide"] > 0 and st["exact_tests"] > 0, st
